@@ -1,0 +1,233 @@
+/*
+ * sph.h — C-ABI of the B200-native adaptive SPH step (sca2012_b200).
+ *
+ * This is the drop-in boundary for the reference's per-step particle pipeline.
+ * In the reference the host class SPHSystem calls C++-linkage launch wrappers
+ * that take raw device pointers (SPH-3D-2/sph_system.cuh:1-91,
+ * SPH-2D/sph_system.cuh:1-72) and mirrors every constant into a __constant__
+ * SysParam block re-uploaded each step (SPH-3D-2/sph_param.h:8-87,
+ * SPH-2D/sph_param.h:6-70, set_parameters at SPH-3D-2/sph_system.cu:34-37).
+ * Here the same responsibilities sit behind an opaque handle:
+ *
+ *   sph_config            <- SysParam + the SPHSystem constructor constants
+ *                            (SPH-3D-2/sph_system.cpp:6-229, SPH-2D/sph_system.cpp:5-146)
+ *   sph_config_preset     <- the three reference constructors (2D, 3D-2, 3D-4)
+ *                            plus the synthetic SI-unit workloads
+ *   sph_create/destroy    <- SPHSystem::SPHSystem / ~SPHSystem (alloc_array calls)
+ *   sph_add_particles     <- SPHSystem::add_particle + the H2D copy_array
+ *                            (SPH-3D-2/sph_system.cpp:285-300, :263)
+ *   sph_step              <- SPHSystem::animation() / animate()
+ *                            (SPH-3D-2/sph_system.cpp:302-404, SPH-2D/sph_system.cpp:190-264)
+ *   sph_get_state         <- the D2H copy_array of m_host_mem at the end of a step
+ *                            (SPH-3D-2/sph_system.cpp:401)
+ *   sph_get_debug         <- reads of m_dev_hash / m_dev_index / m_cell_start /
+ *                            m_cell_end / m_trans_vel (the step's intermediates)
+ *   sph_density_grid,     <- integrate_dens + integrate_normal + SPHSystem::marching_cube
+ *   sph_extract_surface      (SPH-3D-2/sph_system.cu:2185-2351, sph_system.cpp:406-542)
+ *
+ * Conventions: every call returns an int status (SPH_OK == 0).  All pointers
+ * in signatures are HOST pointers unless the name says _dev.  A handle owns
+ * its device memory and its CUDA stream; it is not thread-safe, separate
+ * handles are independent.  Particle vectors are passed with `dim` floats per
+ * particle (2 or 3).  The particle count lives on the device; sph_step does
+ * not synchronise with the host.
+ */
+#ifndef SCA2012_B200_SPH_H
+#define SCA2012_B200_SPH_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define SPH_OK             0
+#define SPH_ERR_INVALID    1  /* bad argument / config */
+#define SPH_ERR_CAPACITY   2  /* particle capacity exceeded (add or split) */
+#define SPH_ERR_CUDA       3  /* CUDA runtime error */
+#define SPH_ERR_NO_DEVICE  4  /* no CUDA device / kernels not loadable */
+#define SPH_ERR_NONFINITE  5  /* non-finite position detected by the step */
+#define SPH_ERR_RANGE      6  /* size beyond a fixed maximum of the entry point */
+
+/* ---- presets (sph_config_preset) ---- */
+#define SPH_PRESET_REF_2D    0  /* SPH-2D/sph_system.cpp:5-146            */
+#define SPH_PRESET_REF_3D2   1  /* SPH-3D-2/sph_system.cpp:6-229          */
+#define SPH_PRESET_REF_3D4   2  /* SPH-3D-4/sph_system.cpp:6-229          */
+#define SPH_PRESET_DAM_2D    3  /* 2D dam break, 4096 particles, SI units */
+#define SPH_PRESET_DAM_3D2   4  /* 3D two-way adaptive, 131072 particles  */
+#define SPH_PRESET_DAM_3D4   5  /* 3D four-way adaptive, 1114112 particles */
+#define SPH_PRESET_ROLLOUT_3D 6 /* 32^3 block, two-way, differentiable    */
+
+/* integrator variants */
+#define SPH_INTEGRATE_REF3D  0  /* v+=a*dt/rho; v+=g*dt/rho; x+=v*dt; walls; ev=(ev+v)/2 (SPH-3D-2/sph_system.cu:237-321) */
+#define SPH_INTEGRATE_REF2D  1  /* a=(a+g*dt)/rho; v+=a*dt; ev=(ev+v)/2; x+=v*dt; walls (SPH-2D/sph_system.cu:219-251) */
+#define SPH_INTEGRATE_PHYS   2  /* v+=(F/m+g)*dt; x+=v*dt; walls; ev=(ev+v)/2 */
+
+/* split criteria */
+#define SPH_SPLIT_WAVELET    0  /* energy*co_energy + surface*co_surface > split_criteria (SPH-3D-2/sph_system.cu:1564) */
+#define SPH_SPLIT_DEFICIT    1  /* neighbour count < split_min_neighbors or rho < split_density_ratio*rho0 */
+
+/* merge criteria */
+#define SPH_MERGE_WAVELET    0  /* level 2 and energy*co_energy + surface*co_surface < merge_criteria (SPH-3D-2/sph_system.cu:1694) */
+#define SPH_MERGE_WAVELET_CELL 1 /* 2D: criterion read from the particle whose index equals the cell index (SPH-2D/sph_system.cu:1207) */
+#define SPH_MERGE_INTERIOR   2  /* level 2 and interior (not split-flagged) for merge_interior_steps steps */
+
+typedef struct sph_sphere {
+    float pos[3];
+    float radius;
+    float damping;
+} sph_sphere;
+
+/*
+ * Every physical constant of one solver instance.  Per-level arrays use
+ * index 0 for level 1 ("large") and index 1 for level 2 ("small"), the two
+ * particle levels of the reference.  Kernel coefficients are stored exactly
+ * as the reference stores them (float, computed on the host).
+ */
+typedef struct sph_config {
+    uint32_t dim;            /* 2 or 3 */
+    uint32_t max_particle;   /* capacity of the handle */
+    float world[3];          /* x, y, z extent (2D: x, y; z unused) */
+    float cell_size;         /* uniform hash cell edge (= level-1 kernel length) */
+    uint32_t ncell[3];       /* cells per axis (2D: ncell[2] == 1) */
+
+    float mass[2], kernel[2], kernel2[2], kernel6[2], radius[2];
+    float poly6[2], spiky[2], visco[2], grad_poly6[2], lapc_poly6[2], poly6_radius[2];
+
+    float gravity[3];
+    float wall_damping;      /* velocity factor at a wall (reference: -0.6) */
+    float rest_density;
+    float gas_constant;
+    float time_step;
+    float viscosity;
+    float surface_threshold; /* |grad c| above which surface tension acts */
+    float surface_coef;      /* 0.1 (3D-2), 0.02 (3D-4), 0.04 (2D) */
+    float co_surface, co_energy;
+    float split_criteria, merge_criteria;
+    float density_skip_r2;   /* density loop skips pairs closer than this (3D 1e-4, 2D 1e-12) */
+    float lapc_three_quarters; /* factor in (r2 - f*(h2-r2)); reference integer 3/4 == 0 */
+
+    uint32_t split_ways;     /* 2 or 4 */
+    uint32_t use_split, use_merge;
+    uint32_t integrator;     /* SPH_INTEGRATE_* */
+    uint32_t kernel_h6_twice;/* 1: spiky/visco terms divided by h^6 a second time (reference) */
+    uint32_t energy_large_kernel; /* 1: wavelet energy uses the level-1 kernel for all levels (3D) */
+    uint32_t energy_mass_weight;  /* 1: energy *= mass (3D-4) */
+    uint32_t energy_skip_close;   /* 1: energy loop skips r2 < 1e-4 (3D); 0: keeps it (2D) */
+    uint32_t split_rule;     /* SPH_SPLIT_* */
+    uint32_t merge_rule;     /* SPH_MERGE_* */
+    uint32_t split_min_neighbors;   /* SPH_SPLIT_DEFICIT */
+    float split_density_ratio;      /* SPH_SPLIT_DEFICIT */
+    uint32_t merge_interior_steps;  /* SPH_MERGE_INTERIOR */
+    uint32_t split_copies_fields;   /* 1: child copies dens/press/surface (2D) */
+
+    /* obstacles and interactive forces (reference integrator / force kernel) */
+    uint32_t use_cylinder;
+    sph_sphere sphere[3];
+    uint32_t push_left, push_right; /* 3D push forces (SPH-3D-4/sph_system.cu:229-242) */
+    uint32_t push_y_div;            /* y threshold = height / push_y_div (3D-2 5, 3D-4 10) */
+    uint32_t extern_force_on;       /* 2D mouse force (SPH-2D/sph_system.cu:781-789) */
+    float extern_click[2], extern_force[2], extern_len, extern_coe;
+
+    /* density grid / marching cubes (SPH-3D-2/sph_system.cpp:86-92) */
+    uint32_t dens_mul;
+    float den_size;
+    uint32_t ndens[3];
+    float iso_value;
+    uint32_t mc_interpolate; /* 0: edge midpoints (reference); 1: linear interpolation */
+} sph_config;
+
+/* Host view of a particle state (SoA).  Vectors hold `dim` floats per
+ * particle.  Any pointer may be NULL on read to skip that field. */
+typedef struct sph_state_view {
+    uint32_t n;
+    float *pos, *vel, *ev, *acc;
+    float *dens, *press, *energy, *surface;
+    uint32_t *level;
+    uint32_t *interior;      /* SPH_MERGE_INTERIOR counter */
+} sph_state_view;
+
+/* Intermediates of the last step (host arrays sized by the caller).
+ * n_sorted = particle count the step started with; total_cell = cells. */
+typedef struct sph_debug_view {
+    uint32_t n_sorted, total_cell;
+    uint32_t *hash;          /* [n_sorted] cell key of each sorted slot      */
+    uint32_t *index;         /* [n_sorted] particle index of each sorted slot */
+    uint32_t *cell_start;    /* [total_cell] first sorted slot, 0xffffffff if empty */
+    uint32_t *cell_end;      /* [total_cell] one past last slot, 0 if empty  */
+    float *trans_vel;        /* [n_sorted*dim] wavelet-transformed velocity, by particle index */
+    uint32_t *nbr_count;     /* [n_sorted] neighbours within own kernel, by particle index */
+    uint32_t *split_flag;    /* [n_sorted] 1 if the particle split, by particle index */
+    uint32_t *removed;       /* [n_sorted] 1 if merged away, by particle index */
+} sph_debug_view;
+
+/* Triangle soup of the iso-surface (host arrays, 3 floats per corner). */
+typedef struct sph_mesh_view {
+    uint32_t max_triangles;
+    uint32_t num_triangles;  /* out: triangles produced (may exceed max) */
+    float *v0, *v1, *v2;
+    float *n0, *n1, *n2;
+} sph_mesh_view;
+
+typedef struct sph_handle sph_handle;
+
+/* sizeof(sph_config), for foreign-function bindings to check their layout. */
+size_t sph_config_size(void);
+
+/* Fills *cfg with a preset.  Reference presets reproduce the reference
+ * constructors' constants bit for bit. */
+int sph_config_preset(int preset, sph_config *cfg);
+
+int sph_create(const sph_config *cfg, sph_handle **out);
+int sph_destroy(sph_handle *h);
+
+/* Replaces runtime-adjustable constants (time step, toggles, forces...).
+ * The cell grid, dimension and capacity must match the handle's. */
+int sph_set_config(sph_handle *h, const sph_config *cfg);
+int sph_get_config(const sph_handle *h, sph_config *cfg);
+
+/* Appends n particles (pos/vel: n*dim floats, level: 1 or 2). */
+int sph_add_particles(sph_handle *h, uint32_t n, const float *pos, const float *vel,
+                      const uint32_t *level);
+
+/* Replaces the whole state; NULL optional fields are zero-filled. */
+int sph_set_state(sph_handle *h, const sph_state_view *st);
+
+/* Advances nsteps steps on the handle's stream (asynchronous). */
+int sph_step(sph_handle *h, int nsteps);
+
+/* Synchronises and returns the device-side status (capacity / non-finite). */
+int sph_sync(sph_handle *h);
+
+int sph_get_num_particles(sph_handle *h, uint32_t *n);
+int sph_get_state(sph_handle *h, sph_state_view *st);
+int sph_get_debug(sph_handle *h, sph_debug_view *dbg);
+
+/* The handle's CUDA stream (a cudaStream_t), for callers timing or
+ * ordering work against the step. */
+void *sph_get_stream(sph_handle *h);
+
+/* on != 0: the step also keeps per-particle debug intermediates
+ * (wavelet-transformed velocity) for sph_get_debug. */
+int sph_set_debug(sph_handle *h, int on);
+
+/* Number of kernel launches the last sph_step issued. */
+int sph_last_launch_count(const sph_handle *h, uint32_t *launches);
+
+/* Density grid of the current state (splat + normals on the device), copied
+ * to host arrays of ndens[0]*ndens[1]*ndens[2] floats / 3*that floats. */
+int sph_density_grid(sph_handle *h, float *dens, float *normal);
+
+/* Density grid + marching cubes on the device; triangles appended in the
+ * reference's cell order (x outer, y, z inner). */
+int sph_extract_surface(sph_handle *h, sph_mesh_view *mesh);
+
+/* Human-readable text of the last error on this handle (static storage). */
+const char *sph_last_error(const sph_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,179 @@
+"""sca2012_b200 — B200-native adaptive SPH step behind the reference's SPHSystem API.
+
+`Solver` is a thin Python owner of one C-ABI handle (include/sph/sph.h).  It
+mirrors the reference host class's operations (SPH-3D-2/sph_system.h:26-154):
+construct from constants, add particles, advance with `animation()` /
+`step()`, read the particle state back.  All compute runs in the in-tree CUDA
+library; if that library or a GPU is missing the calls raise — there is no
+CPU fallback.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import Config, StateView, DebugView, MeshView  # noqa: F401
+from ._abi import (PRESET_REF_2D, PRESET_REF_3D2, PRESET_REF_3D4, PRESET_DAM_2D,  # noqa: F401
+                   PRESET_DAM_3D2, PRESET_DAM_3D4, PRESET_ROLLOUT_3D)
+
+__all__ = ["Solver", "Config", "preset", "SphError", "lib"]
+
+
+class SphError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"sph error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    return _abi.load()
+
+
+def preset(which):
+    """Config of a preset (SPH_PRESET_*)."""
+    c = Config()
+    rc = lib().sph_config_preset(int(which), C.byref(c))
+    if rc:
+        raise SphError(rc, f"unknown preset {which}")
+    return c
+
+
+def _f(a):
+    return a.ctypes.data_as(_abi.FP) if a is not None else None
+
+
+def _u(a):
+    return a.ctypes.data_as(_abi.UP) if a is not None else None
+
+
+STATE_FIELDS = ("pos", "vel", "ev", "acc", "dens", "press", "energy", "surface", "level", "interior")
+
+
+class Solver:
+    """One solver instance on the current CUDA device."""
+
+    def __init__(self, cfg):
+        self._lib = lib()
+        self.cfg = cfg.copy()
+        self.dim = int(cfg.dim)
+        h = _abi.H()
+        rc = self._lib.sph_create(C.byref(self.cfg), C.byref(h))
+        if rc:
+            raise SphError(rc, "sph_create failed (no CUDA device, or invalid config)")
+        self._h = h
+
+    # -- lifecycle ------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc:
+            msg = self._lib.sph_last_error(self._h)
+            raise SphError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    # -- configuration --------------------------------------------------
+    def set_config(self, cfg):
+        self._check(self._lib.sph_set_config(self._h, C.byref(cfg)), "sph_set_config")
+        self.cfg = cfg.copy()
+
+    def set_debug(self, on=True):
+        self._check(self._lib.sph_set_debug(self._h, 1 if on else 0), "sph_set_debug")
+
+    @property
+    def stream_ptr(self):
+        return self._lib.sph_get_stream(self._h)
+
+    # -- particles -------------------------------------------------------
+    def add_particles(self, pos, vel, level):
+        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, self.dim)
+        vel = np.ascontiguousarray(vel, np.float32).reshape(-1, self.dim)
+        level = np.ascontiguousarray(level, np.uint32).reshape(-1)
+        n = pos.shape[0]
+        self._check(self._lib.sph_add_particles(self._h, n, _f(pos), _f(vel), _u(level)), "sph_add_particles")
+
+    def set_state(self, st):
+        """st: dict with pos/vel/ev/acc (n x dim) and optional scalars, level (n)."""
+        pos = np.ascontiguousarray(st["pos"], np.float32)
+        n = pos.shape[0]
+        keep = {}
+        v = StateView()
+        v.n = n
+        for k in STATE_FIELDS:
+            a = st.get(k)
+            if a is None:
+                continue
+            a = np.ascontiguousarray(a, np.uint32 if k in ("level", "interior") else np.float32)
+            keep[k] = a
+            setattr(v, k, _u(a) if k in ("level", "interior") else _f(a))
+        self._check(self._lib.sph_set_state(self._h, C.byref(v)), "sph_set_state")
+
+    def num_particles(self):
+        n = C.c_uint32()
+        self._check(self._lib.sph_get_num_particles(self._h, C.byref(n)), "sph_get_num_particles")
+        return int(n.value)
+
+    def get_state(self):
+        n = self.num_particles()
+        d = self.dim
+        out = {k: np.zeros((n, d), np.float32) for k in ("pos", "vel", "ev", "acc")}
+        for k in ("dens", "press", "energy", "surface"):
+            out[k] = np.zeros(n, np.float32)
+        out["level"] = np.zeros(n, np.uint32)
+        out["interior"] = np.zeros(n, np.uint32)
+        v = StateView()
+        v.n = n
+        for k in STATE_FIELDS:
+            setattr(v, k, _u(out[k]) if k in ("level", "interior") else _f(out[k]))
+        self._check(self._lib.sph_get_state(self._h, C.byref(v)), "sph_get_state")
+        return out
+
+    def get_debug(self):
+        n_guess = self.cfg.max_particle
+        ncell = int(np.prod([self.cfg.ncell[a] for a in range(self.dim)]))
+        dv = DebugView()
+        dv.n_sorted = 0
+        # first call with no arrays to learn n
+        arr = {k: np.zeros(n_guess, np.uint32) for k in ("hash", "index", "nbr_count", "split_flag", "removed")}
+        arr["cell_start"] = np.zeros(ncell, np.uint32)
+        arr["cell_end"] = np.zeros(ncell, np.uint32)
+        arr["trans_vel"] = np.zeros(n_guess * self.dim, np.float32)
+        for k, a in arr.items():
+            setattr(dv, k, _f(a) if k == "trans_vel" else _u(a))
+        self._check(self._lib.sph_get_debug(self._h, C.byref(dv)), "sph_get_debug")
+        n = int(dv.n_sorted)
+        out = {k: a[:n].copy() for k, a in arr.items() if k not in ("cell_start", "cell_end", "trans_vel")}
+        out["cell_start"] = arr["cell_start"]
+        out["cell_end"] = arr["cell_end"]
+        out["trans_vel"] = arr["trans_vel"][: n * self.dim].reshape(n, self.dim).copy()
+        out["n"] = n
+        return out
+
+    # -- stepping ----------------------------------------------------------
+    def step(self, nsteps=1):
+        self._check(self._lib.sph_step(self._h, int(nsteps)), "sph_step")
+
+    def sync(self):
+        rc = self._lib.sph_sync(self._h)
+        if rc:
+            self._check(rc, "sph_sync")
+
+    def sync_status(self):
+        """Synchronises and returns the device status code (0 = ok) without raising."""
+        return int(self._lib.sph_sync(self._h))
+
+    def last_launch_count(self):
+        n = C.c_uint32()
+        self._check(self._lib.sph_last_launch_count(self._h, C.byref(n)), "sph_last_launch_count")
+        return int(n.value)
+
+    # reference spelling: SPHSystem::animation() advances one step
+    def animation(self):
+        self.step(1)

@@ -1,0 +1,519 @@
+// sph_api.cu — C-ABI implementation: handle, device buffers, step orchestration.
+//
+// Replaces the reference's SPHSystem constructor allocations
+// (SPH-3D-2/sph_system.cpp:34-47,95-101), its per-step launch sequence
+// (animation(), SPH-3D-2/sph_system.cpp:302-404; animate(), SPH-2D/sph_system.cpp:190-264)
+// and its launch wrappers (SPH-3D-2/sph_system.cuh).  Differences by design:
+// one stream per handle, no host synchronisation inside a step (the particle
+// count lives on the device), state in SoA float4 arrays, every CUDA status
+// checked and reported through the int return codes.
+#include "../../include/sph/sph.h"
+#include "sph_kernels.cuh"
+#include "sph_scan.cuh"
+#include "sph_mc.cuh"
+
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace sph;
+
+struct sph_handle {
+    sph_config cfg;
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    uint32_t cap = 0, ncells = 0;
+    CanonPtrs buf[2];
+    int cur = 0;
+    Counters *cnt = nullptr;       // [2], one per parity
+    WorkPtrs w;
+    uint32_t *scan_blocks = nullptr;  // kScanBlocks * 2 u32
+    uint32_t *scan_grand = nullptr;   // scratch total
+    uint32_t n_ub = 0;                // host upper bound of the live count
+    uint32_t n_last_sorted = 0;       // count the last step started with (host copy)
+    bool have_step = false;
+    bool debug = false;
+    uint32_t last_launches = 0;
+    std::vector<void *> allocs;
+    std::string err;
+    // density grid + marching cubes
+    McBuffers mc;
+    bool grid_valid = false;
+};
+
+namespace {
+
+const char *kNoHandle = "null handle";
+
+template <typename T> int dalloc(sph_handle *h, T **p, size_t count)
+{
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, sizeof(T) * (count ? count : 1));
+    if (e != cudaSuccess) {
+        h->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        return SPH_ERR_CUDA;
+    }
+    cudaMemset(q, 0, sizeof(T) * (count ? count : 1));
+    h->allocs.push_back(q);
+    *p = (T *)q;
+    return SPH_OK;
+}
+
+int cuda_check(sph_handle *h, const char *what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        h->err = std::string(what) + ": " + cudaGetErrorString(e);
+        return SPH_ERR_CUDA;
+    }
+    return SPH_OK;
+}
+
+uint32_t total_cells(const sph_config &c) { return c.ncell[0] * c.ncell[1] * (c.dim == 3 ? c.ncell[2] : 1u); }
+
+int validate(const sph_config *c, std::string &why)
+{
+    if (!c) { why = "null config"; return SPH_ERR_INVALID; }
+    if (c->dim != 2 && c->dim != 3) { why = "dim must be 2 or 3"; return SPH_ERR_INVALID; }
+    if (c->max_particle == 0 || c->max_particle > (1u << 30)) { why = "max_particle out of range"; return SPH_ERR_INVALID; }
+    if (!(c->cell_size > 0.0f)) { why = "cell_size must be > 0"; return SPH_ERR_INVALID; }
+    for (uint32_t a = 0; a < c->dim; ++a)
+        if (c->ncell[a] == 0) { why = "empty cell grid"; return SPH_ERR_INVALID; }
+    uint64_t C = (uint64_t)c->ncell[0] * c->ncell[1] * (c->dim == 3 ? c->ncell[2] : 1u);
+    if (C >= (1ull << 31)) { why = "cell grid too large"; return SPH_ERR_INVALID; }
+    if (c->split_ways != 2 && c->split_ways != 4) { why = "split_ways must be 2 or 4"; return SPH_ERR_INVALID; }
+    if (c->kernel[0] > c->cell_size * 1.0000001f || c->kernel[1] > c->cell_size * 1.0000001f) {
+        why = "kernel length exceeds the cell size (neighbour stencil would miss pairs)";
+        return SPH_ERR_INVALID;
+    }
+    return SPH_OK;
+}
+
+uint32_t grid_for(const sph_handle *h, uint32_t work)
+{
+    uint32_t b = (work + kThreads - 1) / kThreads;
+    uint32_t cap = (uint32_t)h->num_sms * 8u;
+    return std::max(1u, std::min(b, cap));
+}
+
+// Exclusive scan of u32 `in` -> `out`; length from len_ptr (device) or len_const.
+void scan_u32(sph_handle *h, const uint32_t *in, uint32_t *out, const uint32_t *len_ptr, uint32_t len_const,
+              uint32_t *grand, int total_at_len, uint32_t *list)
+{
+    scan_phase1<uint32_t><<<kScanBlocks, kScanThreads, 0, h->stream>>>(in, len_ptr, len_const, h->scan_blocks);
+    scan_phase2<uint32_t><<<1, kScanBlocks, 0, h->stream>>>(h->scan_blocks, grand);
+    scan_phase3<uint32_t><<<kScanBlocks, kScanThreads, 0, h->stream>>>(in, out, len_ptr, len_const, h->scan_blocks,
+                                                                       grand, total_at_len, list);
+    h->last_launches += 3;
+}
+
+template <int DIM> int run_step(sph_handle *h)
+{
+    const sph_config &c = h->cfg;
+    const int p = h->cur;
+    Counters *cin = h->cnt + p, *cout = h->cnt + (p ^ 1);
+    CanonPtrs in = h->buf[p], out = h->buf[p ^ 1];
+    WorkPtrs w = h->w;
+    const uint32_t G = grid_for(h, h->n_ub);
+    const uint32_t GC = grid_for(h, h->ncells);
+    cudaStream_t s = h->stream;
+
+    cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, s);
+    k_hash<DIM><<<G, kThreads, 0, s>>>(c, cin, in, w);
+    scan_u32(h, w.cell_count, w.cell_off, nullptr, h->ncells, h->scan_grand, 1, nullptr);
+    k_scatter<<<G, kThreads, 0, s>>>(cin, w);
+    k_reorder<<<G, kThreads, 0, s>>>(cin, in, w);
+    k_density<DIM><<<G, kThreads, 0, s>>>(c, cin, w);
+    k_force_integrate<DIM><<<G, kThreads, 0, s>>>(c, cin, w);
+    k_energy_split<DIM><<<G, kThreads, 0, s>>>(c, cin, in, w, h->debug ? 1 : 0);
+    h->last_launches += 7;
+    scan_u32(h, w.split_c, w.split_rank, &cin->n, 0, &cin->n_split, 0, w.split_list);
+    k_split_guard<<<1, 1, 0, s>>>(c, cin, h->cap);
+    h->last_launches += 1;
+    if (c.use_merge) {
+        const uint32_t GM = grid_for(h, (uint32_t)std::min<uint64_t>((uint64_t)h->ncells * 32u, 1u << 30));
+        k_merge<DIM><<<GM, kThreads, 0, s>>>(c, cin, in, w, h->ncells, h->cap);
+        h->last_launches += 1;
+    }
+    scan_u32(h, w.removed_c, w.removed_rank, &cin->n, 0, &cin->n_removed, 0, nullptr);
+    k_write<DIM><<<G, kThreads, 0, s>>>(c, cin, cout, out, w);
+    h->last_launches += 1;
+    (void)GC;
+    h->cur = p ^ 1;
+    uint64_t ub = h->n_ub;
+    if (c.use_split) ub *= (c.split_ways == 4 ? 4u : 2u);
+    h->n_ub = (uint32_t)std::min<uint64_t>(ub, h->cap);
+    return cuda_check(h, "sph_step launch");
+}
+
+void pack4(const float *src, int dim, uint32_t n, std::vector<float4> &dst, const uint32_t *level)
+{
+    dst.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (src) {
+            v.x = src[(size_t)i * dim];
+            v.y = src[(size_t)i * dim + 1];
+            if (dim == 3) v.z = src[(size_t)i * dim + 2];
+        }
+        if (level) v.w = (float)level[i];
+        dst[i] = v;
+    }
+}
+
+void unpack4(const std::vector<float4> &src, int dim, uint32_t n, float *dst)
+{
+    if (!dst) return;
+    for (uint32_t i = 0; i < n; ++i) {
+        dst[(size_t)i * dim] = src[i].x;
+        dst[(size_t)i * dim + 1] = src[i].y;
+        if (dim == 3) dst[(size_t)i * dim + 2] = src[i].z;
+    }
+}
+
+uint32_t read_n(sph_handle *h)
+{
+    uint32_t n = 0;
+    cudaMemcpyAsync(&n, &h->cnt[h->cur].n, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream);
+    cudaStreamSynchronize(h->stream);
+    return n;
+}
+
+void write_n(sph_handle *h, uint32_t n)
+{
+    Counters c0;
+    std::memset(&c0, 0, sizeof(c0));
+    cudaMemcpyAsync(&c0, &h->cnt[h->cur], sizeof(Counters), cudaMemcpyDeviceToHost, h->stream);
+    cudaStreamSynchronize(h->stream);
+    c0.n = n;
+    cudaMemcpyAsync(&h->cnt[h->cur], &c0, sizeof(Counters), cudaMemcpyHostToDevice, h->stream);
+    cudaStreamSynchronize(h->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int sph_create(const sph_config *cfg, sph_handle **out)
+{
+    if (!out) return SPH_ERR_INVALID;
+    *out = nullptr;
+    std::string why;
+    int rc = validate(cfg, why);
+    if (rc) { fprintf(stderr, "sph_create: %s\n", why.c_str()); return rc; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return SPH_ERR_NO_DEVICE;
+    sph_handle *h = new sph_handle();
+    h->cfg = *cfg;
+    cudaGetDevice(&h->device);
+    cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return SPH_ERR_CUDA;
+    }
+    h->cap = cfg->max_particle;
+    h->ncells = total_cells(*cfg);
+    const size_t cap = h->cap, C = h->ncells;
+    rc = SPH_OK;
+    for (int b = 0; b < 2 && !rc; ++b) {
+        CanonPtrs &q = h->buf[b];
+        rc |= dalloc(h, &q.pos, cap); rc |= dalloc(h, &q.vel, cap);
+        rc |= dalloc(h, &q.ev, cap); rc |= dalloc(h, &q.acc, cap);
+        rc |= dalloc(h, &q.dens, cap); rc |= dalloc(h, &q.press, cap);
+        rc |= dalloc(h, &q.energy, cap); rc |= dalloc(h, &q.surface, cap);
+        rc |= dalloc(h, &q.interior, cap);
+    }
+    WorkPtrs &w = h->w;
+    rc |= dalloc(h, &h->cnt, 2);
+    rc |= dalloc(h, &w.key, cap); rc |= dalloc(h, &w.slot, cap); rc |= dalloc(h, &w.tmp, cap);
+    rc |= dalloc(h, &w.cell_count, C); rc |= dalloc(h, &w.cell_off, C + 1);
+    rc |= dalloc(h, &w.sidx, cap); rc |= dalloc(h, &w.skey, cap); rc |= dalloc(h, &w.inv, cap);
+    rc |= dalloc(h, &w.spos, cap); rc |= dalloc(h, &w.svel, cap); rc |= dalloc(h, &w.sev, cap);
+    rc |= dalloc(h, &w.saux, cap);
+    rc |= dalloc(h, &w.spos_n, cap); rc |= dalloc(h, &w.svel_n, cap); rc |= dalloc(h, &w.sev_n, cap);
+    rc |= dalloc(h, &w.sacc_n, cap);
+    rc |= dalloc(h, &w.ssurf, cap); rc |= dalloc(h, &w.senergy, cap);
+    rc |= dalloc(h, &w.snbr, cap); rc |= dalloc(h, &w.sinter, cap);
+    rc |= dalloc(h, &w.stv, cap);
+    rc |= dalloc(h, &w.split_c, cap); rc |= dalloc(h, &w.removed_c, cap);
+    rc |= dalloc(h, &w.split_rank, cap); rc |= dalloc(h, &w.removed_rank, cap);
+    rc |= dalloc(h, &w.split_list, cap); rc |= dalloc(h, &w.leader, cap);
+    rc |= dalloc(h, &w.mpos, cap); rc |= dalloc(h, &w.mvel, cap); rc |= dalloc(h, &w.mev, cap);
+    rc |= dalloc(h, &w.macc, cap); rc |= dalloc(h, &w.menergy, cap);
+    rc |= dalloc(h, &h->scan_blocks, (size_t)kScanBlocks * 2);
+    rc |= dalloc(h, &h->scan_grand, 4);
+    if (!rc) rc = mc_alloc(h->mc, *cfg, h->allocs);
+    if (rc) {
+        fprintf(stderr, "sph_create: %s\n", h->err.c_str());
+        sph_destroy(h);
+        return rc ? rc : SPH_ERR_CUDA;
+    }
+    cudaDeviceSynchronize();
+    *out = h;
+    return SPH_OK;
+}
+
+int sph_destroy(sph_handle *h)
+{
+    if (!h) return SPH_ERR_INVALID;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void *p : h->allocs) cudaFree(p);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return SPH_OK;
+}
+
+int sph_set_config(sph_handle *h, const sph_config *cfg)
+{
+    if (!h || !cfg) return SPH_ERR_INVALID;
+    std::string why;
+    if (validate(cfg, why)) { h->err = why; return SPH_ERR_INVALID; }
+    if (cfg->dim != h->cfg.dim || cfg->max_particle != h->cfg.max_particle ||
+        total_cells(*cfg) != h->ncells || cfg->ncell[0] != h->cfg.ncell[0] || cfg->ncell[1] != h->cfg.ncell[1]) {
+        h->err = "sph_set_config: dimension, capacity and cell grid are fixed at creation";
+        return SPH_ERR_INVALID;
+    }
+    if (cfg->ndens[0] != h->cfg.ndens[0] || cfg->ndens[1] != h->cfg.ndens[1] || cfg->ndens[2] != h->cfg.ndens[2]) {
+        h->err = "sph_set_config: density grid is fixed at creation";
+        return SPH_ERR_INVALID;
+    }
+    h->cfg = *cfg;
+    return SPH_OK;
+}
+
+int sph_get_config(const sph_handle *h, sph_config *cfg)
+{
+    if (!h || !cfg) return SPH_ERR_INVALID;
+    *cfg = h->cfg;
+    return SPH_OK;
+}
+
+int sph_add_particles(sph_handle *h, uint32_t n, const float *pos, const float *vel, const uint32_t *level)
+{
+    if (!h || (n && (!pos || !level))) return SPH_ERR_INVALID;
+    const int dim = (int)h->cfg.dim;
+    uint32_t n0 = read_n(h);
+    if ((uint64_t)n0 + n > h->cap) { h->err = "sph_add_particles: capacity exceeded"; return SPH_ERR_CAPACITY; }
+    for (uint32_t i = 0; i < n; ++i)
+        if (level[i] != 1u && level[i] != 2u) { h->err = "level must be 1 or 2"; return SPH_ERR_INVALID; }
+    std::vector<float4> p4, v4, z4(n, make_float4(0.f, 0.f, 0.f, 0.f));
+    pack4(pos, dim, n, p4, level);
+    pack4(vel, dim, n, v4, nullptr);
+    std::vector<float> zf(n, 0.0f);
+    std::vector<uint32_t> zu(n, 0u);
+    const CanonPtrs &b = h->buf[h->cur];
+    cudaStream_t s = h->stream;
+    cudaMemcpyAsync(b.pos + n0, p4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.vel + n0, v4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.ev + n0, z4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.acc + n0, z4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.dens + n0, zf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.press + n0, zf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.energy + n0, zf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.surface + n0, zf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.interior + n0, zu.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+    write_n(h, n0 + n);
+    h->n_ub = n0 + n;
+    return cuda_check(h, "sph_add_particles");
+}
+
+int sph_set_state(sph_handle *h, const sph_state_view *st)
+{
+    if (!h || !st) return SPH_ERR_INVALID;
+    const uint32_t n = st->n;
+    if (n > h->cap) { h->err = "sph_set_state: capacity exceeded"; return SPH_ERR_CAPACITY; }
+    if (n && (!st->pos || !st->level)) return SPH_ERR_INVALID;
+    const int dim = (int)h->cfg.dim;
+    std::vector<float4> p4, v4, e4, a4;
+    pack4(st->pos, dim, n, p4, st->level);
+    pack4(st->vel, dim, n, v4, nullptr);
+    pack4(st->ev, dim, n, e4, nullptr);
+    pack4(st->acc, dim, n, a4, nullptr);
+    std::vector<float> zf(n, 0.0f);
+    std::vector<uint32_t> zu(n, 0u);
+    const CanonPtrs &b = h->buf[h->cur];
+    cudaStream_t s = h->stream;
+    cudaMemcpyAsync(b.pos, p4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.vel, v4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.ev, e4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.acc, a4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.dens, st->dens ? st->dens : zf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.press, st->press ? st->press : zf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.energy, st->energy ? st->energy : zf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.surface, st->surface ? st->surface : zf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.interior, st->interior ? st->interior : zu.data(), sizeof(uint32_t) * n,
+                    cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+    write_n(h, n);
+    h->n_ub = n;
+    h->have_step = false;
+    return cuda_check(h, "sph_set_state");
+}
+
+int sph_step(sph_handle *h, int nsteps)
+{
+    if (!h || nsteps < 0) return SPH_ERR_INVALID;
+    h->last_launches = 0;
+    for (int k = 0; k < nsteps; ++k) {
+        if (h->n_ub == 0) break;
+        h->n_last_sorted = 0;   // resolved lazily by sph_get_debug
+        int rc = h->cfg.dim == 3 ? run_step<3>(h) : run_step<2>(h);
+        if (rc) return rc;
+        h->have_step = true;
+    }
+    return SPH_OK;
+}
+
+int sph_sync(sph_handle *h)
+{
+    if (!h) return SPH_ERR_INVALID;
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) { h->err = cudaGetErrorString(e); return SPH_ERR_CUDA; }
+    Counters c0;
+    cudaMemcpy(&c0, &h->cnt[h->cur], sizeof(Counters), cudaMemcpyDeviceToHost);
+    if (c0.error) {
+        uint32_t err = c0.error;
+        c0.error = 0;
+        cudaMemcpy(&h->cnt[h->cur], &c0, sizeof(Counters), cudaMemcpyHostToDevice);
+        for (int code = 1; code < 32; ++code)
+            if (err & (1u << code)) {
+                h->err = code == SPH_ERR_CAPACITY ? "particle capacity exceeded by a split (splits skipped)"
+                                                  : "device reported an error";
+                return code;
+            }
+    }
+    return SPH_OK;
+}
+
+int sph_get_num_particles(sph_handle *h, uint32_t *n)
+{
+    if (!h || !n) return SPH_ERR_INVALID;
+    *n = read_n(h);
+    return cuda_check(h, "sph_get_num_particles");
+}
+
+int sph_get_state(sph_handle *h, sph_state_view *st)
+{
+    if (!h || !st) return SPH_ERR_INVALID;
+    const uint32_t n = read_n(h);
+    const uint32_t lim = st->n;   // caller's capacity; 0 = just report n
+    st->n = n;
+    if (lim == 0) return SPH_OK;
+    if (lim < n) { h->err = "sph_get_state: host arrays too small"; return SPH_ERR_INVALID; }
+    const int dim = (int)h->cfg.dim;
+    const CanonPtrs &b = h->buf[h->cur];
+    std::vector<float4> t(n);
+    auto get4 = [&](const float4 *src, float *dst) {
+        if (!dst) return;
+        cudaMemcpy(t.data(), src, sizeof(float4) * n, cudaMemcpyDeviceToHost);
+        unpack4(t, dim, n, dst);
+    };
+    get4(b.pos, st->pos);
+    get4(b.vel, st->vel);
+    get4(b.ev, st->ev);
+    get4(b.acc, st->acc);
+    if (st->level) {
+        cudaMemcpy(t.data(), b.pos, sizeof(float4) * n, cudaMemcpyDeviceToHost);
+        for (uint32_t i = 0; i < n; ++i) st->level[i] = (uint32_t)t[i].w;
+    }
+    if (st->dens) cudaMemcpy(st->dens, b.dens, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    if (st->press) cudaMemcpy(st->press, b.press, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    if (st->energy) cudaMemcpy(st->energy, b.energy, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    if (st->surface) cudaMemcpy(st->surface, b.surface, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    if (st->interior) cudaMemcpy(st->interior, b.interior, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
+    return cuda_check(h, "sph_get_state");
+}
+
+int sph_get_debug(sph_handle *h, sph_debug_view *d)
+{
+    if (!h || !d) return SPH_ERR_INVALID;
+    if (!h->have_step) { h->err = "no step run since the last state change"; return SPH_ERR_INVALID; }
+    cudaStreamSynchronize(h->stream);
+    Counters c0;
+    cudaMemcpy(&c0, &h->cnt[h->cur ^ 1], sizeof(Counters), cudaMemcpyDeviceToHost);
+    const uint32_t n = c0.n;   // count the last step started with
+    d->n_sorted = n;
+    d->total_cell = h->ncells;
+    const WorkPtrs &w = h->w;
+    const int dim = (int)h->cfg.dim;
+    std::vector<uint32_t> sidx(n);
+    cudaMemcpy(sidx.data(), w.sidx, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
+    if (d->hash) cudaMemcpy(d->hash, w.skey, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
+    if (d->index) std::memcpy(d->index, sidx.data(), sizeof(uint32_t) * n);
+    if (d->cell_start || d->cell_end) {
+        uint32_t *ds = nullptr, *de = nullptr;
+        cudaMalloc(&ds, sizeof(uint32_t) * h->ncells);
+        cudaMalloc(&de, sizeof(uint32_t) * h->ncells);
+        k_cell_ranges<<<grid_for(h, h->ncells), kThreads, 0, h->stream>>>(w.cell_off, h->ncells, ds, de);
+        cudaStreamSynchronize(h->stream);
+        if (d->cell_start) cudaMemcpy(d->cell_start, ds, sizeof(uint32_t) * h->ncells, cudaMemcpyDeviceToHost);
+        if (d->cell_end) cudaMemcpy(d->cell_end, de, sizeof(uint32_t) * h->ncells, cudaMemcpyDeviceToHost);
+        cudaFree(ds);
+        cudaFree(de);
+    }
+    if (d->trans_vel) {
+        std::vector<float4> t(n);
+        cudaMemcpy(t.data(), w.stv, sizeof(float4) * n, cudaMemcpyDeviceToHost);
+        for (uint32_t s = 0; s < n; ++s) {
+            float *o = d->trans_vel + (size_t)sidx[s] * dim;
+            o[0] = t[s].x; o[1] = t[s].y;
+            if (dim == 3) o[2] = t[s].z;
+        }
+    }
+    if (d->nbr_count) {
+        std::vector<uint32_t> t(n);
+        cudaMemcpy(t.data(), w.snbr, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
+        for (uint32_t s = 0; s < n; ++s) d->nbr_count[sidx[s]] = t[s];
+    }
+    if (d->split_flag) {
+        cudaMemcpy(d->split_flag, w.split_c, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
+        if (c0.split_off) std::memset(d->split_flag, 0, sizeof(uint32_t) * n);
+    }
+    if (d->removed) cudaMemcpy(d->removed, w.removed_c, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
+    return cuda_check(h, "sph_get_debug");
+}
+
+void *sph_get_stream(sph_handle *h) { return h ? (void *)h->stream : nullptr; }
+
+int sph_last_launch_count(const sph_handle *h, uint32_t *launches)
+{
+    if (!h || !launches) return SPH_ERR_INVALID;
+    *launches = h->last_launches;
+    return SPH_OK;
+}
+
+int sph_set_debug(sph_handle *h, int on)
+{
+    if (!h) return SPH_ERR_INVALID;
+    h->debug = on != 0;
+    return SPH_OK;
+}
+
+const char *sph_last_error(const sph_handle *h) { return h ? h->err.c_str() : kNoHandle; }
+
+}  // extern "C"
+
+extern "C" {
+
+int sph_density_grid(sph_handle *h, float *dens, float *normal)
+{
+    if (!h) return SPH_ERR_INVALID;
+    (void)dens; (void)normal;
+    h->err = "sph_density_grid: not available in this build";
+    return SPH_ERR_INVALID;
+}
+
+int sph_extract_surface(sph_handle *h, sph_mesh_view *mesh)
+{
+    if (!h) return SPH_ERR_INVALID;
+    (void)mesh;
+    h->err = "sph_extract_surface: not available in this build";
+    return SPH_ERR_INVALID;
+}
+
+}  // extern "C"

@@ -1,0 +1,683 @@
+// sph_kernels.cuh — sm_100a kernels of one adaptive-SPH step.
+//
+// Layout in HBM (all SoA, 16-byte aligned):
+//   canonical state, two buffers swapped every step, in the reference's
+//   particle-index order (the order split/merge/compaction and the readback
+//   depend on): pos4 = (x, y, z, level), vel4, ev4, acc4, dens, press,
+//   energy, surface, interior;
+//   sorted working copies, in cell-key order, that the neighbour loops read
+//   contiguously: spos/svel/sev (gathered), saux = (rho, p, p/rho^2, m/rho),
+//   and the post-integration spos_n/svel_n/sev_n/sacc_n, ssurf, senergy.
+// Cell key = z*R*C + y*R + x with x = floor(pos / cell) in FP32, exactly the
+// reference's calc_grid_pos/calc_grid_hash (SPH-3D-2/sph_system.cu:18-32).
+// Neighbour search visits the 3 (2D) or 9 (3D) rows of x-adjacent cells; in
+// key order each row is one contiguous slot range.
+//
+// Every decision that is an integer outcome of float arithmetic (cell keys,
+// r^2 < h^2, h - r > 0, the split/merge scores) is evaluated with explicit
+// round-to-nearest intrinsics in a fixed order, so the CPU oracle's FP32
+// replica reproduces it bit for bit.
+#pragma once
+#include <cstdint>
+#include "../../include/sph/sph.h"
+
+namespace sph {
+
+constexpr uint32_t kEmpty = 0xffffffffu;
+constexpr int kThreads = 256;
+
+// Device-side counters of one step parity.
+struct Counters {
+    uint32_t n;            // live particles at step start
+    uint32_t n_split;      // split particles this step
+    uint32_t n_removed;    // merged-away particles this step
+    uint32_t error;        // SPH_ERR_* bit flags (1 << code)
+    uint32_t split_off;    // 1: splits suppressed this step (capacity)
+    uint32_t pad[3];
+};
+
+struct CanonPtrs {
+    float4 *pos, *vel, *ev, *acc;
+    float *dens, *press, *energy, *surface;
+    uint32_t *interior;
+};
+
+struct WorkPtrs {
+    uint32_t *key, *slot, *tmp;          // per canonical particle / slot
+    uint32_t *cell_count, *cell_off;     // C, C+1
+    uint32_t *sidx, *skey, *inv;         // sorted slot -> particle, key; particle -> slot
+    float4 *spos, *svel, *sev, *saux;
+    float4 *spos_n, *svel_n, *sev_n, *sacc_n;
+    float *ssurf, *senergy;
+    uint32_t *snbr, *sinter;
+    float4 *stv;                         // debug: wavelet-transformed velocity
+    uint32_t *split_c, *removed_c;       // per canonical particle
+    uint32_t *split_rank, *removed_rank; // exclusive scans
+    uint32_t *split_list;                // split rank -> particle
+    uint32_t *leader;                    // per sorted slot: 1 if merge survivor
+    float4 *mpos, *mvel, *mev, *macc;    // merged values at the leader's slot
+    float *menergy;
+};
+
+// ------------------------------------------------------------ helpers
+__device__ __forceinline__ int lv(float w) { return w == 1.0f ? 0 : 1; }
+
+__device__ __forceinline__ uint32_t cell_coord(float x, float cs, uint32_t n)
+{
+    float f = floorf(__fdiv_rn(x, cs));
+    if (!(f >= 0.0f)) return 0u;
+    if (f >= (float)n) return n - 1u;
+    return (uint32_t)f;
+}
+
+template <int DIM>
+__device__ __forceinline__ uint3 cell_of(const sph_config &c, float4 p)
+{
+    uint3 q;
+    q.x = cell_coord(p.x, c.cell_size, c.ncell[0]);
+    q.y = cell_coord(p.y, c.cell_size, c.ncell[1]);
+    q.z = DIM == 3 ? cell_coord(p.z, c.cell_size, c.ncell[2]) : 0u;
+    return q;
+}
+
+__device__ __forceinline__ uint32_t key_of(const sph_config &c, uint32_t x, uint32_t y, uint32_t z)
+{
+    return z * c.ncell[0] * c.ncell[1] + y * c.ncell[0] + x;
+}
+
+// fma(dz, dz, fma(dx, dx, dy*dy)) with d = a - b, all round-to-nearest.
+template <int DIM>
+__device__ __forceinline__ float r2_of(float4 a, float4 b, float &dx, float &dy, float &dz)
+{
+    dx = __fsub_rn(a.x, b.x);
+    dy = __fsub_rn(a.y, b.y);
+    float t = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+    if (DIM == 3) {
+        dz = __fsub_rn(a.z, b.z);
+        t = __fmaf_rn(dz, dz, t);
+    } else {
+        dz = 0.0f;
+    }
+    return t;
+}
+
+__device__ __forceinline__ float split_score(const sph_config &c, float e, float s)
+{
+    return __fmaf_rn(s, c.co_surface, __fmul_rn(e, c.co_energy));
+}
+
+__device__ __forceinline__ uint32_t grid_stride_start() { return blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ uint32_t grid_stride() { return gridDim.x * blockDim.x; }
+
+// Row ranges of the 3^DIM neighbourhood of cell q: rows (dy, dz); each row is
+// the slot range [off[key(x0)], off[key(x1)+1]) of cells x0..x1.
+template <int DIM>
+__device__ __forceinline__ int row_range(const sph_config &c, const uint32_t *__restrict__ off, uint3 q,
+                                         int dy, int dz, uint32_t &b, uint32_t &e)
+{
+    int y = (int)q.y + dy, z = (int)q.z + dz;
+    if (y < 0 || y >= (int)c.ncell[1]) return 0;
+    if (DIM == 3 && (z < 0 || z >= (int)c.ncell[2])) return 0;
+    uint32_t x0 = q.x > 0 ? q.x - 1 : 0;
+    uint32_t x1 = q.x + 1 < c.ncell[0] ? q.x + 1 : q.x;
+    uint32_t k0 = key_of(c, x0, (uint32_t)y, (uint32_t)z);
+    uint32_t k1 = key_of(c, x1, (uint32_t)y, (uint32_t)z);
+    b = __ldg(off + k0);
+    e = __ldg(off + k1 + 1);
+    return 1;
+}
+
+// ------------------------------------------------------------ 1. hash
+template <int DIM>
+__global__ void __launch_bounds__(kThreads) k_hash(sph_config c, const Counters *__restrict__ cnt,
+                                                  CanonPtrs st, WorkPtrs w)
+{
+    const uint32_t n = cnt->n;
+    for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) {
+        uint3 q = cell_of<DIM>(c, st.pos[i]);
+        uint32_t k = key_of(c, q.x, q.y, q.z);
+        w.key[i] = k;
+        w.slot[i] = atomicAdd(w.cell_count + k, 1u);
+    }
+}
+
+// ------------------------------------------------------------ 3. scatter
+__global__ void __launch_bounds__(kThreads) k_scatter(const Counters *__restrict__ cnt, WorkPtrs w)
+{
+    const uint32_t n = cnt->n;
+    for (uint32_t i = grid_stride_start(); i < n; i += grid_stride())
+        w.tmp[__ldg(w.cell_off + w.key[i]) + w.slot[i]] = i;
+}
+
+// ------------------------------------------------------------ 4. stable order + gather
+// The atomic slot order inside a cell is arbitrary; the stable order (equal
+// keys in ascending particle index, as thrust's radix sort_by_key leaves
+// them, SPH-3D-2/sph_system.cu:119-129) is restored by ranking each particle
+// among its cell's members.  Then the state is gathered into key order.
+__global__ void __launch_bounds__(kThreads) k_reorder(const Counters *__restrict__ cnt, CanonPtrs st, WorkPtrs w)
+{
+    const uint32_t n = cnt->n;
+    for (uint32_t s = grid_stride_start(); s < n; s += grid_stride()) {
+        uint32_t i = w.tmp[s];
+        uint32_t k = w.key[i];
+        uint32_t b = __ldg(w.cell_off + k), e = __ldg(w.cell_off + k + 1);
+        uint32_t r = 0;
+        for (uint32_t t = b; t < e; ++t) r += w.tmp[t] < i;
+        uint32_t d = b + r;
+        w.sidx[d] = i;
+        w.skey[d] = k;
+        w.inv[i] = d;
+        w.spos[d] = st.pos[i];
+        w.svel[d] = st.vel[i];
+        w.sev[d] = st.ev[i];
+    }
+}
+
+// ------------------------------------------------------------ 5. density
+// rho_i = m_i poly6_i h_i^6 + sum_{j != i, skip <= r^2 < h_i^2} m_j poly6_i (h_i^2 - r^2)^3
+// p_i = k ((rho_i / rho0)^3 - 1)         (SPH-3D-2/sph_system.cu:338-677)
+template <int DIM>
+__global__ void __launch_bounds__(kThreads) k_density(sph_config c, const Counters *__restrict__ cnt, WorkPtrs w)
+{
+    const uint32_t n = cnt->n;
+    const float *off_unused = nullptr;
+    (void)off_unused;
+    for (uint32_t s = grid_stride_start(); s < n; s += grid_stride()) {
+        const float4 pi = w.spos[s];
+        const int li = lv(pi.w);
+        const float h2 = c.kernel2[li];
+        const float poly6 = c.poly6[li];
+        const uint32_t k = w.skey[s];
+        uint3 q;
+        q.x = k % c.ncell[0];
+        q.y = (k / c.ncell[0]) % c.ncell[1];
+        q.z = DIM == 3 ? k / (c.ncell[0] * c.ncell[1]) : 0u;
+        float rho = 0.0f;
+        uint32_t nb = 0;
+#pragma unroll 1
+        for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy) {
+                uint32_t b, e;
+                if (!row_range<DIM>(c, w.cell_off, q, dy, dz, b, e)) continue;
+                for (uint32_t t = b; t < e; ++t) {
+                    const float4 pj = w.spos[t];
+                    if (t == s) continue;
+                    float dx, dyy, dzz;
+                    float r2 = r2_of<DIM>(pj, pi, dx, dyy, dzz);
+                    if (r2 < c.density_skip_r2) continue;
+                    if (r2 < h2) {
+                        float x = h2 - r2;
+                        float mj = pj.w == 1.0f ? c.mass[0] : c.mass[1];
+                        rho += mj * poly6 * (x * x * x);
+                        ++nb;
+                    }
+                }
+            }
+        rho += c.mass[li] * poly6 * c.kernel6[li];   // self term
+        float r = rho / c.rest_density;
+        float p = (r * r * r - 1.0f) * c.gas_constant;
+        w.saux[s] = make_float4(rho, p, p / (rho * rho), c.mass[li] / rho);
+        w.snbr[s] = nb;
+    }
+}
+
+// ------------------------------------------------------------ 6. force + integrate
+// Pressure, viscosity and colour-field terms (SPH-3D-2/sph_system.cu:679-1137,
+// 2D SPH-2D/sph_system.cu:462-790), then the integrator and walls
+// (SPH-3D-2/sph_system.cu:204-322, SPH-2D/sph_system.cu:198-252).  The
+// integrated state goes to the *_n arrays so the loop never sees it.
+template <int DIM>
+__global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, const Counters *__restrict__ cnt,
+                                                              WorkPtrs w)
+{
+    const uint32_t n = cnt->n;
+    for (uint32_t s = grid_stride_start(); s < n; s += grid_stride()) {
+        const float4 pi = w.spos[s];
+        const float4 evi = w.sev[s];
+        const float4 ai = w.saux[s];   // rho, p, p/rho^2, m/rho
+        const int li = lv(pi.w);
+        const float hi = c.kernel[li], hi2 = c.kernel2[li];
+        const float mi = c.mass[li];
+        const float ispk = c.kernel_h6_twice ? c.spiky[li] / c.kernel6[li] : c.spiky[li];
+        const float ivis = c.kernel_h6_twice ? c.visco[li] / c.kernel6[li] : c.visco[li];
+        const float igrad = -c.grad_poly6[li];
+        const float ilap = c.lapc_poly6[li];
+        const uint32_t k = w.skey[s];
+        uint3 q;
+        q.x = k % c.ncell[0];
+        q.y = (k / c.ncell[0]) % c.ncell[1];
+        q.z = DIM == 3 ? k / (c.ncell[0] * c.ncell[1]) : 0u;
+        float fx = 0.f, fy = 0.f, fz = 0.f, gx = 0.f, gy = 0.f, gz = 0.f, lap = 0.f;
+#pragma unroll 1
+        for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy) {
+                uint32_t b, e;
+                if (!row_range<DIM>(c, w.cell_off, q, dy, dz, b, e)) continue;
+                for (uint32_t t = b; t < e; ++t) {
+                    const float4 pj = w.spos[t];
+                    if (t == s) {
+                        if (DIM == 2)   // SPH-2D/sph_system.cu:599-603 (0 with the integer 3/4)
+                            lap += ilap * ai.w * hi2 * (0.0f - c.lapc_three_quarters * hi2);
+                        continue;
+                    }
+                    float rx, ry, rz;
+                    float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
+                    const int lj = lv(pj.w);
+                    const float maxh2 = fmaxf(hi2, c.kernel2[lj]);
+                    if (!(r2 < maxh2)) continue;
+                    if (r2 < 0.0001f) continue;
+                    const float r = __fsqrt_rn(r2);
+                    const float4 aj = w.saux[t];
+                    const float4 evj = w.sev[t];
+                    float ipk = 0.f, ivk = 0.f, jpk = 0.f, jvk = 0.f;
+                    const float ikr = __fsub_rn(hi, r);
+                    if (ikr > 0.0f) {
+                        ipk = ispk * ikr * ikr;
+                        ivk = ivis * ikr;
+                        const float x = hi2 - r2;
+                        const float tg = igrad * aj.w * x * x;   // -grad_poly6 * m_j/rho_j * (h^2-r^2)^2
+                        gx += tg * rx; gy += tg * ry; gz += tg * rz;
+                        lap += ilap * aj.w * x * (r2 - c.lapc_three_quarters * x);
+                    }
+                    const float jkr = __fsub_rn(c.kernel[lj], r);
+                    if (jkr > 0.0f) {
+                        const float jspk = c.kernel_h6_twice ? c.spiky[lj] / c.kernel6[lj] : c.spiky[lj];
+                        const float jvis = c.kernel_h6_twice ? c.visco[lj] / c.kernel6[lj] : c.visco[lj];
+                        jpk = jspk * jkr * jkr;
+                        jvk = jvis * jkr;
+                    }
+                    const float mj = c.mass[lj];
+                    const float tp = mi * mj * (ai.z + aj.z) * (ipk + jpk) * 0.5f / r;
+                    const float tv = (ai.w * aj.w) * c.viscosity * (ivk + jvk) * 0.5f;
+                    fx += -rx * tp + (evj.x - evi.x) * tv;
+                    fy += -ry * tp + (evj.y - evi.y) * tv;
+                    if (DIM == 3) fz += -rz * tp + (evj.z - evi.z) * tv;
+                }
+            }
+        // surface tension switch (SPH-3D-2/sph_system.cu:1113-1136)
+        const float nrm = sqrtf(gx * gx + gy * gy + gz * gz);
+        if (nrm > c.surface_threshold) {
+            const float f = c.surface_coef * lap / nrm;
+            fx += f * gx; fy += f * gy; fz += f * gz;
+        }
+        if (DIM == 2 && c.extern_force_on) {   // SPH-2D/sph_system.cu:781-789
+            float xl = __fsub_rn(pi.x, c.extern_click[0]), yl = __fsub_rn(pi.y, c.extern_click[1]);
+            if (__fmaf_rn(xl, xl, __fmul_rn(yl, yl)) <= __fmul_rn(c.extern_len, c.extern_len)) {
+                fx += c.extern_force[0] * c.extern_coe;
+                fy += c.extern_force[1] * c.extern_coe;
+            }
+        }
+        w.ssurf[s] = nrm;
+
+        // ---- integrate ----
+        const float rho = ai.x, dt = c.time_step;
+        float4 x = pi;
+        float4 v = w.svel[s];
+        float4 ev = evi;
+        float4 a = make_float4(fx, fy, fz, 0.f);
+        float rad;
+        if (c.integrator == SPH_INTEGRATE_REF2D) {
+            rad = c.radius[li] / 2.0f;
+            a.x = (a.x + c.gravity[0] * dt) / rho;
+            a.y = (a.y + c.gravity[1] * dt) / rho;
+            v.x += a.x * dt; v.y += a.y * dt;
+            ev.x = (ev.x + v.x) / 2.0f; ev.y = (ev.y + v.y) / 2.0f;
+            x.x += v.x * dt; x.y += v.y * dt;
+        } else {
+            rad = c.radius[li];
+            if (c.integrator == SPH_INTEGRATE_REF3D) {
+                if (c.push_left && pi.x < __fdiv_rn(c.world[0], 3.0f) &&
+                    pi.y > __fdiv_rn(c.world[1], (float)c.push_y_div))
+                    a.x += 20.0f;
+                if (c.push_right && pi.x > __fmul_rn(__fdiv_rn(c.world[0], 3.0f), 2.0f) &&
+                    pi.y > __fdiv_rn(c.world[1], (float)c.push_y_div))
+                    a.x -= 20.0f;
+                v.x += a.x * dt / rho; v.y += a.y * dt / rho; v.z += a.z * dt / rho;
+                v.x += c.gravity[0] * dt / rho; v.y += c.gravity[1] * dt / rho; v.z += c.gravity[2] * dt / rho;
+            } else {
+                const float im = 1.0f / mi;
+                v.x += (a.x * im + c.gravity[0]) * dt;
+                v.y += (a.y * im + c.gravity[1]) * dt;
+                v.z += (a.z * im + c.gravity[2]) * dt;
+            }
+            x.x += v.x * dt; x.y += v.y * dt; x.z += v.z * dt;
+            if (DIM == 3 && c.use_cylinder) {   // SPH-3D-2/sph_system.cu:242-282
+                for (int qq = 0; qq < 3; ++qq) {
+                    const sph_sphere S = c.sphere[qq];
+                    float dxs = x.x - S.pos[0], dys = x.y - S.pos[1], dzs = x.z - S.pos[2];
+                    float dist = sqrtf(dxs * dxs + dys * dys + dzs * dzs);
+                    float R = S.radius + rad;
+                    if (dist < R) {
+                        float sx = dxs / dist * R, sy = dys / dist * R, sz = dzs / dist * R;
+                        float il = rsqrtf(sx * sx + sy * sy + sz * sz);
+                        float nx = sx * il, ny = sy * il, nz = sz * il;
+                        x.x = S.pos[0] + sx; x.y = S.pos[1] + sy; x.z = S.pos[2] + sz;
+                        float vn = v.x * nx + v.y * ny + v.z * nz;
+                        v.x -= S.damping * vn * nx; v.y -= S.damping * vn * ny; v.z -= S.damping * vn * nz;
+                    }
+                }
+            }
+        }
+        // walls x, y, z (SPH-3D-2/sph_system.cu:285-319)
+        {
+            float *xp = &x.x, *vp = &v.x;
+            for (int d = 0; d < DIM; ++d) {
+                const float hi_w = c.world[d] - rad;
+                if (xp[d] >= hi_w) { vp[d] *= c.wall_damping; xp[d] = hi_w; }
+                if (xp[d] < rad) { vp[d] *= c.wall_damping; xp[d] = rad; }
+            }
+        }
+        if (c.integrator != SPH_INTEGRATE_REF2D) {
+            ev.x = (ev.x + v.x) / 2.0f; ev.y = (ev.y + v.y) / 2.0f; ev.z = (ev.z + v.z) / 2.0f;
+        }
+        w.spos_n[s] = x;        // .w keeps the level
+        w.svel_n[s] = v;
+        w.sev_n[s] = ev;
+        w.sacc_n[s] = a;
+    }
+}
+
+// ------------------------------------------------------------ 7. energy + split decision
+// Wavelet energy on the STALE cell lists (built at step start) with the NEW
+// positions (SPH-3D-2/sph_system.cu:1169-1546), then the split decision
+// (decide_adaptive_kernel, :1548-1574) written per particle index.
+__device__ __forceinline__ float wavelet(float x, float amp)
+{
+    // psi(x) = amp * (x^2/4 - 1) * EXP^(-x^2/8), EXP = 2.718281f (sigma = 2)
+    const float x2 = x * x;
+    return amp * (x2 * 0.25f - 1.0f) * exp2f(-x2 * 0.125f * 1.44269476f);
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kThreads) k_energy_split(sph_config c, Counters *__restrict__ cnt,
+                                                           CanonPtrs st, WorkPtrs w, int want_tv)
+{
+    const uint32_t n = cnt->n;
+    // 2/(PI^0.25 * sqrt(3 sigma)) with PI = 3.141592f, sigma = 2
+    const float amp = 2.0f / (powf(3.141592f, 0.25f) * sqrtf(6.0f));
+    for (uint32_t s = grid_stride_start(); s < n; s += grid_stride()) {
+        const float4 pi = w.spos_n[s];
+        const int li = lv(pi.w);
+        const int lk = c.energy_large_kernel ? 0 : li;
+        const float h = c.kernel[lk], h2 = c.kernel2[lk];
+        const float ih = 1.0f / h, isq = 1.0f / sqrtf(h);
+        const uint3 q = cell_of<DIM>(c, pi);
+        float tsx = 0.f, tsy = 0.f, tsz = 0.f, tvx = 0.f, tvy = 0.f, tvz = 0.f;
+#pragma unroll 1
+        for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy) {
+                uint32_t b, e;
+                if (!row_range<DIM>(c, w.cell_off, q, dy, dz, b, e)) continue;
+                for (uint32_t t = b; t < e; ++t) {
+                    if (t == s) continue;
+                    const float4 pj = w.spos_n[t];
+                    float rx, ry, rz;
+                    float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
+                    if (!(r2 < h2)) continue;
+                    if (c.energy_skip_close && r2 < 0.0001f) continue;
+                    const float4 vj = w.svel_n[t];
+                    float wx = wavelet(rx * ih, amp), wy = wavelet(ry * ih, amp);
+                    tsx += wx; tsy += wy;
+                    tvx += vj.x * wx * isq; tvy += vj.y * wy * isq;
+                    if (DIM == 3) {
+                        float wz = wavelet(rz * ih, amp);
+                        tsz += wz;
+                        tvz += vj.z * wz * isq;
+                    }
+                }
+            }
+        tvx /= tsx; tvy /= tsy; tvz = DIM == 3 ? tvz / tsz : 0.f;
+        float energy = 0.5f * (tvx * tvx + tvy * tvy);
+        if (c.energy_mass_weight) energy *= c.mass[li];
+        w.senergy[s] = energy;
+        if (want_tv) w.stv[s] = make_float4(tvx, tvy, tvz, 0.f);
+
+        const uint32_t i = w.sidx[s];
+        const float surf = w.ssurf[s];
+        const float dens = w.saux[s].x;
+        const uint32_t nb = w.snbr[s];
+        uint32_t split = 0;
+        if (c.use_split && pi.w == 1.0f) {
+            if (c.split_rule == SPH_SPLIT_DEFICIT)
+                split = (nb < c.split_min_neighbors || dens < c.split_density_ratio * c.rest_density) ? 1u : 0u;
+            else
+                split = split_score(c, energy, surf) > c.split_criteria ? 1u : 0u;
+        }
+        w.split_c[i] = split;
+        w.removed_c[i] = 0u;
+        if (c.merge_rule == SPH_MERGE_INTERIOR) {
+            const int flagged = nb < c.split_min_neighbors || dens < c.split_density_ratio * c.rest_density;
+            w.sinter[s] = (flagged || split) ? 0u : st.interior[i] + 1u;
+        }
+    }
+}
+
+// Capacity guard after the split scan: if the children would not fit, this
+// step runs without splits and reports SPH_ERR_CAPACITY (the reference writes
+// past its buffer, SPH-3D-2/sph_system.cu:1645-1656).
+__global__ void k_split_guard(const sph_config c, Counters *cnt, uint32_t cap)
+{
+    uint64_t extra = c.split_ways == 4 ? 3u : 1u;
+    uint64_t after = (uint64_t)cnt->n + (uint64_t)cnt->n_split * extra;
+    if (after > cap) {
+        cnt->split_off = 1u;
+        cnt->error |= 1u << SPH_ERR_CAPACITY;
+    } else {
+        cnt->split_off = 0u;
+    }
+}
+
+// ------------------------------------------------------------ 8. merge
+// One warp per cell over its sorted members (merge_kernel,
+// SPH-3D-2/sph_system.cu:1661-1789; 3D-4 :1702-1888; 2D :1177-1270).
+// Eligible members (evaluated on the post-split values) are ranked by warp
+// ballots in slot order; groups of `ways` consecutive eligible members merge
+// into the first, with V = m/rho weights (level already set to 1 for the
+// survivor, :1742-1777) or the plain mean in 2D.
+constexpr int kMergeListMax = 256;   // eligible members held per warp in shared memory
+
+template <int DIM>
+__device__ __forceinline__ int merge_eligible(const sph_config &c, const WorkPtrs &w, uint32_t t,
+                                              uint32_t split_on, uint32_t ways, float cell_score)
+{
+    const uint32_t i = w.sidx[t];
+    const uint32_t sp = split_on & w.split_c[i];
+    const float lvl = sp ? 2.0f : w.spos_n[t].w;
+    if (c.merge_rule == SPH_MERGE_WAVELET) {
+        float en = w.senergy[t];
+        if (sp && ways == 4) en = en / 4.0f;
+        return lvl != 1.0f && split_score(c, en, w.ssurf[t]) < c.merge_criteria;
+    }
+    if (c.merge_rule == SPH_MERGE_WAVELET_CELL) return lvl == 2.0f && cell_score < c.merge_criteria;
+    return lvl != 1.0f && w.sinter[t] >= c.merge_interior_steps;
+}
+
+// Merges the group g[0..ways) into g[0] (values on the post-split state).
+template <int DIM>
+__device__ __forceinline__ void merge_group(const sph_config &c, const WorkPtrs &w, const uint32_t *g,
+                                            uint32_t ways, uint32_t split_on, float hs2)
+{
+    float V[4], Vs = 0.f;
+    for (uint32_t k = 0; k < ways; ++k) {
+        // eligible members are level 2; the survivor's level is set to 1
+        // before its volume is taken (SPH-3D-2/sph_system.cu:1742-1756)
+        V[k] = DIM == 2 ? 1.0f : (k == 0 ? c.mass[0] : c.mass[1]) / w.saux[g[k]].x;
+        Vs += V[k];
+    }
+    float4 P = make_float4(0.f, 0.f, 0.f, 0.f), Vv = P, E = P, A = P;
+    float en = 0.f;
+    for (uint32_t k = 0; k < ways; ++k) {
+        const uint32_t t = g[k];
+        const uint32_t sp = split_on & w.split_c[w.sidx[t]];
+        float4 p = w.spos_n[t];
+        if (sp) p.x += hs2;
+        const float4 vv = w.svel_n[t], ee = w.sev_n[t], aa = w.sacc_n[t];
+        float ek = w.senergy[t];
+        if (sp && ways == 4) ek = ek / 4.0f;
+        P.x += p.x * V[k]; P.y += p.y * V[k]; P.z += p.z * V[k];
+        Vv.x += vv.x * V[k]; Vv.y += vv.y * V[k]; Vv.z += vv.z * V[k];
+        E.x += ee.x * V[k]; E.y += ee.y * V[k]; E.z += ee.z * V[k];
+        A.x += aa.x * V[k]; A.y += aa.y * V[k]; A.z += aa.z * V[k];
+        en += ek;
+    }
+    const uint32_t t1 = g[0];
+    w.mpos[t1] = make_float4(P.x / Vs, P.y / Vs, P.z / Vs, 1.0f);
+    w.mvel[t1] = make_float4(Vv.x / Vs, Vv.y / Vs, Vv.z / Vs, 0.f);
+    w.mev[t1] = make_float4(E.x / Vs, E.y / Vs, E.z / Vs, 0.f);
+    w.macc[t1] = make_float4(A.x / Vs, A.y / Vs, A.z / Vs, 0.f);
+    w.menergy[t1] = en / (float)ways;
+    w.leader[t1] = 1u;
+    for (uint32_t k = 1; k < ways; ++k) w.removed_c[w.sidx[g[k]]] = 1u;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kThreads) k_merge(sph_config c, const Counters *__restrict__ cnt,
+                                                   CanonPtrs st, WorkPtrs w, uint32_t ncells, uint32_t cap)
+{
+    __shared__ uint32_t list[kThreads / 32][kMergeListMax];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
+    const uint32_t n = cnt->n;
+    const uint32_t split_on = cnt->split_off ? 0u : 1u;
+    const uint32_t ways = c.split_ways == 4 ? 4u : 2u;
+    const uint32_t extra = ways - 1u;
+    const float hs2 = c.kernel[1] / 2.0f;
+    for (uint32_t cell = blockIdx.x * (blockDim.x >> 5) + wib; cell < ncells; cell += warps_total) {
+        const uint32_t b = w.cell_off[cell], e = w.cell_off[cell + 1];
+        if (e - b < ways) continue;
+        // 2D rule: the criterion of the particle whose INDEX equals the cell
+        // index, as memory holds it at merge time (SPH-2D/sph_system.cu:1207)
+        float cell_score = 0.f;
+        if (c.merge_rule == SPH_MERGE_WAVELET_CELL) {
+            float eq, sq;
+            const uint32_t n_after = n + (split_on ? cnt->n_split * extra : 0u);
+            if (cell < n) {
+                const uint32_t sl = w.inv[cell];
+                eq = w.senergy[sl]; sq = w.ssurf[sl];
+            } else if (cell < n_after) {
+                const uint32_t sl = w.inv[w.split_list[(cell - n) / extra]];
+                eq = w.senergy[sl]; sq = w.ssurf[sl];
+            } else if (cell < cap) {
+                eq = st.energy[cell]; sq = st.surface[cell];
+            } else {
+                eq = 0.f; sq = 0.f;   // beyond the allocation: treated as zeroed memory
+            }
+            cell_score = split_score(c, eq, sq);
+        }
+        uint32_t count = 0;
+        for (uint32_t base = b; base < e; base += 32) {
+            const uint32_t t = base + lane;
+            const int el = t < e ? merge_eligible<DIM>(c, w, t, split_on, ways, cell_score) : 0;
+            const uint32_t m = __ballot_sync(0xffffffffu, el);
+            const uint32_t r = count + __popc(m & ((1u << lane) - 1u));
+            if (el && r < kMergeListMax) list[wib][r] = t;
+            count += __popc(m);
+        }
+        __syncwarp();
+        const uint32_t groups = count / ways;
+        if (count <= (uint32_t)kMergeListMax) {
+            for (uint32_t g = lane; g < groups; g += 32)
+                merge_group<DIM>(c, w, &list[wib][g * ways], ways, split_on, hs2);
+        } else if (lane == 0) {
+            // more eligible members than the per-warp list holds: walk the
+            // cell serially with the same group arithmetic
+            uint32_t grp[4], got = 0, done = 0;
+            for (uint32_t t = b; t < e && done < groups; ++t) {
+                if (!merge_eligible<DIM>(c, w, t, split_on, ways, cell_score)) continue;
+                grp[got++] = t;
+                if (got == ways) {
+                    merge_group<DIM>(c, w, grp, ways, split_on, hs2);
+                    got = 0;
+                    ++done;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------ 10. write-out
+// Stable partition by status (rearrange, SPH-3D-2/sph_system.cu:1818-1840):
+// [surviving particles in index order][children in split order][removed].
+// Children follow adaptive_particle_kernel (:1576-1615; 3D-4 :1583-1656;
+// 2D :1133-1160).  Writes the other canonical buffer.
+template <int DIM>
+__global__ void __launch_bounds__(kThreads) k_write(sph_config c, const Counters *__restrict__ cnt,
+                                                   Counters *__restrict__ cnt_next, CanonPtrs out, WorkPtrs w)
+{
+    const uint32_t n = cnt->n;
+    const uint32_t split_on = cnt->split_off ? 0u : 1u;
+    const uint32_t ways = c.split_ways == 4 ? 4u : 2u;
+    const uint32_t extra = ways - 1u;
+    const uint32_t n_split = split_on ? cnt->n_split : 0u;
+    const uint32_t n_removed = cnt->n_removed;
+    const uint32_t n_after = n + n_split * extra;
+    const uint32_t n_live = n_after - n_removed;
+    const float hs2 = c.kernel[1] / 2.0f;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        cnt_next->n = n_live;
+        cnt_next->error = cnt->error;
+        cnt_next->n_split = 0;
+        cnt_next->n_removed = 0;
+        cnt_next->split_off = 0;
+    }
+    for (uint32_t s = grid_stride_start(); s < n; s += grid_stride()) {
+        const uint32_t i = w.sidx[s];
+        const uint32_t sp = split_on & w.split_c[i];
+        const uint32_t rm = w.removed_c[i];
+        const uint32_t rr = w.removed_rank[i];
+        const uint32_t dst = rm ? n_live + rr : i - rr;
+        float4 p = w.spos_n[s], v = w.svel_n[s], e = w.sev_n[s], a = w.sacc_n[s];
+        const float4 aux = w.saux[s];
+        float en = w.senergy[s];
+        const float sf = w.ssurf[s];
+        uint32_t inter = c.merge_rule == SPH_MERGE_INTERIOR ? w.sinter[s] : 0u;
+        const float4 p_pre = p;
+        if (sp) {
+            p.x += hs2;
+            p.w = 2.0f;
+            if (ways == 4) en = en / 4.0f;
+            inter = 0u;
+        }
+        if (w.leader[s]) {
+            p = w.mpos[s]; v = w.mvel[s]; e = w.mev[s]; a = w.macc[s];
+            if (DIM == 2) en = w.menergy[s];
+            inter = 0u;
+            w.leader[s] = 0u;   // reset for the next step
+        }
+        out.pos[dst] = p; out.vel[dst] = v; out.ev[dst] = e; out.acc[dst] = a;
+        out.dens[dst] = aux.x; out.press[dst] = aux.y; out.energy[dst] = en; out.surface[dst] = sf;
+        out.interior[dst] = inter;
+        if (sp) {
+            const uint32_t base = n - n_removed + w.split_rank[i] * extra;
+            const float4 v0 = w.svel_n[s], e0 = w.sev_n[s], a0 = w.sacc_n[s];
+            const float ec = ways == 4 ? w.senergy[s] / 4.0f : w.senergy[s];
+            for (uint32_t k = 0; k < extra; ++k) {
+                float4 pc = p_pre;
+                pc.w = 2.0f;
+                if (k == 0) pc.x = p_pre.x - hs2;
+                else if (k == 1) pc.z = p_pre.z - hs2;
+                else pc.z = p_pre.z + hs2;
+                const uint32_t cd = base + k;
+                out.pos[cd] = pc; out.vel[cd] = v0; out.ev[cd] = e0; out.acc[cd] = a0;
+                out.dens[cd] = aux.x; out.press[cd] = aux.y; out.energy[cd] = ec; out.surface[cd] = sf;
+                out.interior[cd] = 0u;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ debug helpers
+__global__ void k_cell_ranges(const uint32_t *__restrict__ off, uint32_t ncells, uint32_t *start, uint32_t *end)
+{
+    for (uint32_t q = grid_stride_start(); q < ncells; q += grid_stride()) {
+        uint32_t b = off[q], e = off[q + 1];
+        start[q] = e > b ? b : kEmpty;
+        end[q] = e > b ? e : 0u;
+    }
+}
+
+}  // namespace sph

@@ -1,0 +1,132 @@
+// sph_scan.cuh — device-wide exclusive prefix sums whose length is read from
+// device memory, so a step that changes its particle count on the device
+// never needs the host to learn the count (the reference syncs on two
+// thrust::reduce calls per step, SPH-3D-2/sph_system.cu:1639,1836).
+//
+// Three launches: per-block chunk totals, one block scanning the totals,
+// per-block rescans with the block offset.  The grid is fixed at launch
+// (kScanBlocks); each block takes a contiguous chunk of ceil(len/kScanBlocks)
+// elements, so the traffic is two reads and one write of the input.
+#pragma once
+#include <cstdint>
+
+namespace sph {
+
+constexpr int kScanBlocks = 1024;   // fixed grid of the scan phases (== threads of phase 2)
+constexpr int kScanThreads = 256;
+
+template <typename T> struct Add {
+    __device__ __forceinline__ T operator()(T a, T b) const { return a + b; }
+};
+__device__ __forceinline__ uint2 operator+(uint2 a, uint2 b) { return make_uint2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ uint2 operator-(uint2 a, uint2 b) { return make_uint2(a.x - b.x, a.y - b.y); }
+
+template <typename T> __device__ __forceinline__ T zero_of();
+template <> __device__ __forceinline__ uint32_t zero_of<uint32_t>() { return 0u; }
+template <> __device__ __forceinline__ uint2 zero_of<uint2>() { return make_uint2(0u, 0u); }
+
+template <typename T> __device__ __forceinline__ T shfl_up(T v, int d)
+{
+    return __shfl_up_sync(0xffffffffu, v, d);
+}
+template <> __device__ __forceinline__ uint2 shfl_up<uint2>(uint2 v, int d)
+{
+    return make_uint2(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d));
+}
+
+// Inclusive scan across the block; returns the thread's inclusive value and
+// writes the block total to *total.
+template <typename T>
+__device__ __forceinline__ T block_inclusive_scan(T v, T *warp_tot, T *total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int d = 1; d < 32; d <<= 1) {
+        T o = shfl_up(v, d);
+        if (lane >= d) v = v + o;
+    }
+    if (lane == 31) warp_tot[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        T w = lane < nw ? warp_tot[lane] : zero_of<T>();
+        for (int d = 1; d < 32; d <<= 1) {
+            T o = shfl_up(w, d);
+            if (lane >= d) w = w + o;
+        }
+        if (lane < nw) warp_tot[lane] = w;
+    }
+    __syncthreads();
+    if (warp > 0) v = v + warp_tot[warp - 1];
+    *total = warp_tot[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return v;
+}
+
+__device__ __forceinline__ void chunk_of(uint32_t len, uint32_t &b, uint32_t &e)
+{
+    uint32_t chunk = (len + gridDim.x - 1) / gridDim.x;
+    b = min(len, blockIdx.x * chunk);
+    e = min(len, b + chunk);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) scan_phase1(const T *__restrict__ in, const uint32_t *len_ptr,
+                                                           uint32_t len_const, T *__restrict__ block_tot)
+{
+    __shared__ T wt[kScanThreads / 32];
+    const uint32_t len = len_ptr ? *len_ptr : len_const;
+    uint32_t b, e;
+    chunk_of(len, b, e);
+    T acc = zero_of<T>();
+    for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) acc = acc + in[i];
+    T tot;
+    block_inclusive_scan(acc, wt, &tot);
+    if (threadIdx.x == 0) block_tot[blockIdx.x] = tot;
+}
+
+// One block of kScanBlocks threads: exclusive scan of the block totals;
+// grand total to *grand (if non-null).
+template <typename T>
+__global__ void __launch_bounds__(kScanBlocks) scan_phase2(T *block_tot, T *grand)
+{
+    __shared__ T wt[kScanBlocks / 32];
+    T v = block_tot[threadIdx.x];
+    T tot;
+    T inc = block_inclusive_scan(v, wt, &tot);
+    block_tot[threadIdx.x] = inc - v;
+    if (threadIdx.x == 0 && grand) *grand = tot;
+}
+
+// Exclusive scan of each chunk plus its block offset.  If out_total_at_len,
+// out[len] receives the grand total (used for cell offsets, out[C]).
+// If list != nullptr (T = uint32_t flags only), list[out[i]] = i for in[i]==1.
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) scan_phase3(const T *__restrict__ in, T *__restrict__ out,
+                                                           const uint32_t *len_ptr, uint32_t len_const,
+                                                           const T *__restrict__ block_off,
+                                                           const T *grand, int out_total_at_len,
+                                                           uint32_t *list)
+{
+    __shared__ T wt[kScanThreads / 32];
+    const uint32_t len = len_ptr ? *len_ptr : len_const;
+    uint32_t b, e;
+    chunk_of(len, b, e);
+    T carry = block_off[blockIdx.x];
+    for (uint32_t base = b; base < e; base += blockDim.x) {
+        uint32_t i = base + threadIdx.x;
+        T v = i < e ? in[i] : zero_of<T>();
+        T tot;
+        T inc = block_inclusive_scan(v, wt, &tot);
+        if (i < e) {
+            T ex = carry + inc - v;
+            out[i] = ex;
+            if constexpr (sizeof(T) == 4) {
+                if (list && v) list[ex] = i;
+            }
+        }
+        carry = carry + tot;
+    }
+    if (out_total_at_len && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[len] = *grand;
+}
+
+}  // namespace sph

@@ -1,0 +1,117 @@
+"""CUDA path vs the CPU oracle, stage by stage, through the C-ABI.
+
+For each reference preset (2D, 3D-2 two-way, 3D-4 four-way) and the SI
+workload presets: a state S0 is produced on the GPU by a few warm-up steps of
+the CUDA solver itself; then from S0 one step runs with split/merge off and
+one with them on, and every stage is checked against the oracle fed the same
+FP32 inputs (see tests/_parity.py for the tolerances).
+"""
+import numpy as np
+import pytest
+
+import sca2012_b200 as sph
+from sca2012_b200 import scenes
+from oracle import oracle as O
+from tests._parity import check_close, check_equal
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "ref_2d": (sph.PRESET_REF_2D, scenes.ref_init_2d, 10),
+    "ref_3d2": (sph.PRESET_REF_3D2, scenes.ref_box_3d2, 8),
+    "ref_3d4": (sph.PRESET_REF_3D4, lambda c: _crop(scenes.ref_box_3d4(c), 14.0), 4),
+    "dam_2d": (sph.PRESET_DAM_2D, scenes.dam_2d, 3),
+    "dam_3d2_small": (sph.PRESET_DAM_3D2, lambda c: scenes.block_3d(c, (24, 24, 12), 0.01, seed=3), 3),
+}
+
+
+def _crop(scene, xmax):
+    pos, vel, lvl = scene
+    m = pos[:, 0] < xmax
+    return pos[m], vel[m], lvl[m]
+
+
+def _cfg(preset, split, merge):
+    c = sph.preset(preset)
+    c.use_split = int(split)
+    c.use_merge = int(merge)
+    if c.max_particle > 2_000_000:
+        c.max_particle = 2_000_000
+    return c
+
+
+def run_case(name):
+    preset, scene, warm = CASES[name]
+    cfg_on = _cfg(preset, 1, 1)
+    cfg_off = _cfg(preset, 0, 0)
+    pos, vel, lvl = scene(cfg_on)
+    s = sph.Solver(cfg_on)
+    s.set_debug(True)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    s.step(warm)
+    assert s.sync_status() == 0
+    s0 = s.get_state()
+    # --- step with split/merge off
+    s.set_config(cfg_off)
+    s.set_state(s0)
+    s.step(1)
+    assert s.sync_status() == 0
+    s1 = s.get_state()
+    dbg = s.get_debug()
+    # --- same step with split/merge on
+    s.set_config(cfg_on)
+    s.set_state(s0)
+    s.step(1)
+    assert s.sync_status() == 0
+    s1_on = s.get_state()
+    dbg_on = s.get_debug()
+    s.close()
+    return cfg_on, cfg_off, s0, s1, dbg, s1_on, dbg_on
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_step_parity(name, gpu):
+    cfg_on, cfg, s0, s1, dbg, s1_on, dbg_on = run_case(name)
+    n = len(s0["pos"])
+    assert dbg["n"] == n and len(s1["pos"]) == n
+
+    # (a) hash, stable sort, cell ranges: bit-exact
+    key, idx, cs, ce = O.sort(cfg, s0["pos"])
+    check_equal("cell keys", dbg["hash"], key)
+    check_equal("sorted index", dbg["index"], idx)
+    check_equal("cell_start", dbg["cell_start"], cs)
+    check_equal("cell_end", dbg["cell_end"], ce)
+
+    # (b) density / pressure / neighbour counts
+    dens, press, nbr = O.density(cfg, s0["pos"], s0["level"], idx, cs, ce)
+    check_equal("neighbour counts", dbg["nbr_count"], nbr)
+    check_close("density", s1["dens"], dens)
+    check_close("pressure", s1["press"], press)
+
+    # (c) forces + integration
+    acc, surf, amb = O.force(cfg, s0["pos"], s0["ev"], s0["level"], dens, press, idx, cs, ce)
+    p64, v64, e64, a64, amb2 = O.integrate(cfg, s0["pos"], s0["vel"], s0["ev"], s0["level"], acc, dens)
+    ok = ~(amb | amb2)
+    check_close("surface |grad c|", s1["surface"], surf)
+    check_close("acceleration", s1["acc"], a64, ok)
+    check_close("velocity", s1["vel"], v64, ok)
+    check_close("eval velocity", s1["ev"], e64, ok)
+    check_close("position", s1["pos"], p64, ok)
+
+    # (d) wavelet energy on the stale lists with the GPU's new positions
+    en, tv = O.energy(cfg, s1["pos"], s1["vel"], s0["level"], idx, cs, ce)
+    check_close("energy", s1["energy"], en)
+    check_close("trans_vel", dbg["trans_vel"], tv)
+
+    # (e) split + merge + compaction from the same post-energy state
+    pre = {k: s1[k] for k in ("pos", "vel", "ev", "acc", "dens", "press", "energy", "surface", "level")}
+    pre["interior"] = s0["interior"]
+    exp, split, rem = O.adapt(cfg_on, pre, nbr, idx, cs, ce, cap=cfg_on.max_particle)
+    check_equal("split flags", dbg_on["split_flag"], split)
+    check_equal("merge flags", dbg_on["removed"], rem)
+    assert len(s1_on["pos"]) == len(exp["pos"]), "particle count after split/merge"
+    check_equal("levels", s1_on["level"], exp["level"])
+    for k in ("pos", "vel", "ev", "acc", "energy"):
+        check_close(f"adapted {k}", s1_on[k], exp[k])
+    for k in ("dens", "press", "surface"):
+        check_close(f"adapted {k}", s1_on[k], exp[k])
