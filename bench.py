@@ -1,0 +1,373 @@
+"""Benchmark of the adaptive SPH step (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the 1.1M-particle four-way adaptive configuration): a 128x128x64
+block at spacing 0.005 plus a 65 536-particle sphere falling at 2 m/s in a
+1.28 x 1.28 x 0.64 box (128x128x64 cells of h = 0.01), SI constants
+(rho0 1000, k 3, mu 0.1, dt 2.5e-5), four-way split/merge on.  Synthetic,
+seeded inputs (no dataset exists for this workload).
+
+A step = one call of the C-ABI step: hash, counting sort, stable reorder,
+density, force + integration, wavelet energy + split decision, merge,
+compaction.  `value` = particle-steps/s with the state resident in HBM,
+timed per step with CUDA events on the solver's stream; L2 (126 MB) is
+flushed by a 256 MB write between timed steps, outside the events.  `e2e`
+= the same metric through the host API a reference user calls: each step
+uploads the state from page-locked memory in the reference's Particle
+layout, steps, and reads it back (SPHSystem::animation()'s readback).
+For N > 1 each rank runs an independent replica (the single-scene step has
+no data-parallel split without a halo exchange): weak scaling, value = sum
+of particle-steps / max over ranks of the timed duration.
+
+--impl reference times the CPU oracle (the FP64 port of the reference step)
+on the host cores on the same workload, rank 0 only.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "3D particle-steps/s @1M"
+UNIT = "particle-steps/s"
+WORKLOAD = ("dam_3d4: 1,048,576-particle block (s=0.005) + 65,536-particle sphere, 1.28x1.28x0.64 box, "
+            "128x128x64 cells, four-way split/merge, dt=2.5e-5, SI constants")
+
+# Algorithmic (compulsory) bytes per particle of each stage, every array read
+# or written once (neighbour data re-reads are cache traffic, not counted).
+STAGE_BYTES = {
+    "hash": 16 + 4 + 4 + 4,                  # pos in; key, slot out; count atomics
+    "scatter": 4 + 4 + 4 + 4,                # key, slot, offset in; index out
+    "reorder": 4 + 4 + 48 + 4 + 4 + 4,       # index, key, pos/vel/ev in; sidx, skey, inv out
+    "density": 16 + 16 + 4,                  # pos in; (rho, p, p/rho^2, m/rho), nbr out
+    "force_integrate": 16 * 4 + 16 * 4 + 4,  # pos, ev, aux, vel in; pos, vel, ev, acc, surface out
+    "energy_split": 16 + 16 + 4 + 16 + 4 + 4 + 4 + 4 + 4,  # new pos, vel, surf, aux, nbr, idx; energy, flags
+    "write": 4 * 16 + 16 + 4 * 4 + 4 * 4 + 4 * 16 + 5 * 4,  # sorted state + flags in; canonical state out
+}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--cpu-sample-steps", type=int, default=3)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [r.split(", ") for r in self.lines if r.count(",") >= 8]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------- helpers
+def load_workload(seed):
+    import sca2012_b200 as sph
+    from sca2012_b200 import scenes
+    cfg = sph.preset(sph.PRESET_DAM_3D4)
+    pos, vel, lvl = scenes.dam_3d4(cfg, seed=seed)
+    return cfg, pos, vel, lvl
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def profiled_traffic(stage):
+    """Per-launch DRAM bytes of `stage` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"{stage}_dam3d4.txt")
+    if not os.path.exists(path):
+        return None, None
+    txt = open(path).read()
+    m = re.search(r"traffic_bytes_per_launch_full:\s*([0-9.eE+]+)", txt)
+    n = re.search(r"particles_full:\s*([0-9]+)", txt)
+    return (float(m.group(1)) if m else None), (int(n.group(1)) if n else None)
+
+
+def cpu_baseline(cfg, pos, vel, lvl, steps, threads=None):
+    """The oracle (FP64 port of the reference step) on the host cores."""
+    from oracle import oracle as O
+    if threads:
+        O.set_threads(threads)
+    st = dict(pos=pos, vel=vel, level=lvl)
+    cap = len(pos) * 4
+    t_total, ps = 0.0, 0
+    for _ in range(steps):
+        n = len(st["pos"])
+        t0 = time.perf_counter()
+        st, _ = O.step(cfg, st, cap=cap)
+        t_total += time.perf_counter() - t0
+        ps += n
+    return ps / t_total, O.get_threads(), t_total
+
+
+# ----------------------------------------------------------------- our arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import sca2012_b200 as sph
+    torch.cuda.set_device(local_rank)
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+    cfg, pos, vel, lvl = load_workload(args.seed + rank)
+    n0 = len(pos)
+    s = sph.Solver(cfg)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    stream = torch.cuda.ExternalStream(s.stream_ptr)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def flush_l2():
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+
+    for _ in range(args.warmup):
+        s.step(1)
+    if s.sync_status():
+        raise RuntimeError("solver reported an error during warm-up")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    counts = []
+    launches = 0
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    for k in range(args.steps):
+        flush_l2()
+        counts.append(s.num_particles())   # synchronises; outside the events
+        ev[k][0].record(stream)
+        s.step(1)
+        ev[k][1].record(stream)
+        launches += s.last_launch_count()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    status = s.sync_status()
+    times = [a.elapsed_time(b) for a, b in ev]
+    t_ms = float(sum(times))
+    ps = float(sum(counts))
+    if dist:
+        t = torch.tensor([t_ms], device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        p = torch.tensor([ps], device="cuda", dtype=torch.float64)
+        tdist.all_reduce(p)
+        t_ms, ps = float(t.item()), float(p.item())
+    value = ps / (t_ms * 1e-3)
+
+    # --- per-stage durations (separate profiled steps, same stream)
+    s.set_profiling(True)
+    stage_ms = {}
+    prof_steps = 5
+    n_prof = []
+    for _ in range(prof_steps):
+        flush_l2()
+        n_prof.append(s.num_particles())
+        s.step(1)
+        for name, ms in s.stage_times():
+            stage_ms.setdefault(name, []).append(ms)
+    s.set_profiling(False)
+    stage_avg = {k: float(np.mean(v)) for k, v in stage_ms.items()}
+    top = max(stage_avg, key=stage_avg.get)
+    n_avg = float(np.mean(n_prof))
+    peak, peak_src = measured_peaks()
+    alg = STAGE_BYTES.get(top, 0) * n_avg
+    achieved = alg / (stage_avg[top] * 1e-3) / 1e9
+    traffic_full, n_full = profiled_traffic(top)
+    traffic = traffic_full * (n_avg / n_full) if traffic_full and n_full else None
+
+    # --- plain (non-adaptive) step on the same state, for the "vs plain" ratio
+    plain = cfg.copy()
+    plain.use_split = 0
+    plain.use_merge = 0
+    s.set_config(plain)
+    pt, pc = [], []
+    for _ in range(min(args.steps, 20)):
+        flush_l2()
+        pc.append(s.num_particles())
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        s.step(1)
+        b.record(stream)
+        b.synchronize()
+        pt.append(a.elapsed_time(b))
+    plain_value = sum(pc) / (sum(pt) * 1e-3)
+    s.set_config(cfg)
+
+    # --- end to end through the host API (reference Particle records)
+    rec = s.record_size
+    cap_bytes = cfg.max_particle * rec
+    host = torch.empty(cap_bytes, dtype=torch.uint8, pin_memory=True)
+    n_cur = s.read_particles_into(host.data_ptr(), cap_bytes)
+    e2e_t, e2e_ps, h2d, d2h = 0.0, 0.0, 0, 0
+    e2e_steps = min(args.steps, 20)
+    for _ in range(e2e_steps):
+        flush_l2()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        s.write_particles_from(host.data_ptr(), n_cur)
+        s.step(1)
+        n_next = s.read_particles_into(host.data_ptr(), cap_bytes)
+        b.record(stream)
+        b.synchronize()
+        e2e_t += a.elapsed_time(b)
+        e2e_ps += n_cur
+        h2d += n_cur * rec
+        d2h += n_next * rec + 4
+        n_cur = n_next
+    if dist:
+        t = torch.tensor([e2e_t], device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        p = torch.tensor([e2e_ps], device="cuda", dtype=torch.float64)
+        tdist.all_reduce(p)
+        e2e_t, e2e_ps = float(t.item()), float(p.item())
+    e2e_value = e2e_ps / (e2e_t * 1e-3)
+    status |= s.sync_status()
+    s.close()
+
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            v, cores, tt = cpu_baseline(cfg, pos, vel, lvl, args.cpu_sample_steps)
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                   "sample": f"{args.cpu_sample_steps} full steps of the same workload from its initial state "
+                             f"({tt:.1f} s), FP64 oracle, OpenMP"}
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "particles_initial": n0,
+                       "particles_timed_mean": ps / args.steps / world,
+                       "cells": int(cfg.ncell[0] * cfg.ncell[1] * cfg.ncell[2]),
+                       "l2": "flushed (256 MB write) between timed steps",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "plain_value": plain_value, "adaptive_vs_plain": value / plain_value,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // e2e_steps,
+                    "d2h_bytes_per_step": d2h // e2e_steps,
+                    "api": "sph_write_particles + sph_step + sph_read_particles (page-locked host)"},
+            "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_particle": STAGE_BYTES.get(top),
+                         "launch_ms": stage_avg[top], "peak_source": peak_src,
+                         "note": "neighbour loops are FP32-issue bound: the HBM fraction is low by design"},
+            "stages_ms": stage_avg,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": launches,
+            "status": status,
+        }
+    return out
+
+
+# ----------------------------------------------------------------- reference arm
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    cfg, pos, vel, lvl = load_workload(args.seed)
+    from oracle import oracle as O
+    st = dict(pos=pos, vel=vel, level=lvl)
+    cap = len(pos) * 4
+    # bounded sample: each step is one full oracle step of the workload
+    for _ in range(args.warmup if args.warmup < 2 else 1):
+        st, _ = O.step(cfg, st, cap=cap)
+    t, ps = 0.0, 0.0
+    for _ in range(args.steps):
+        n = len(st["pos"])
+        t0 = time.perf_counter()
+        st, _ = O.step(cfg, st, cap=cap)
+        t += time.perf_counter() - t0
+        ps += n
+    v = ps / t
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "particles_initial": len(pos)},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": O.get_threads(), "kind": "port",
+                             "sample": f"{args.steps} full steps of the workload, FP64 oracle, OpenMP, "
+                                       f"after {min(args.warmup, 1)} warm-up step(s)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank)
+        if out:
+            print(json.dumps(out), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        out = run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as tdist
+            tdist.destroy_process_group()
+    if out:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -205,6 +205,25 @@ int sph_get_num_particles(sph_handle *h, uint32_t *n);
 int sph_get_state(sph_handle *h, sph_state_view *st);
 int sph_get_debug(sph_handle *h, sph_debug_view *dbg);
 
+/* Particle records in the reference's own layout (the Particle class,
+ * SPH-3D-2/sph_system.h:8-24: 72 bytes in 3D; SPH-2D/sph_system.h:7-22:
+ * 56 bytes in 2D).  sph_read_particles is the per-step readback of
+ * SPHSystem::animation() (copy_array(m_host_mem, m_dev_mem, ...),
+ * SPH-3D-2/sph_system.cpp:401); sph_write_particles is the upload after
+ * add_box_particle (:263).  The layout conversion runs on the device; the
+ * host transfer is one contiguous copy (fastest from page-locked memory).
+ * sph_read_particles writes *n_out records (fails if capacity_bytes is too
+ * small). */
+uint32_t sph_particle_record_size(const sph_handle *h);
+int sph_read_particles(sph_handle *h, void *host_dst, uint64_t capacity_bytes, uint32_t *n_out);
+int sph_write_particles(sph_handle *h, const void *host_src, uint32_t n);
+
+/* Per-stage timing: when on, each sph_step records a CUDA event after every
+ * stage; sph_stage_times returns the last step's stage durations (ms) and
+ * names, up to max entries, and the number of stages. */
+int sph_set_profiling(sph_handle *h, int on);
+int sph_stage_times(sph_handle *h, float *ms, const char **names, int max, int *count);
+
 /* The handle's CUDA stream (a cudaStream_t), for callers timing or
  * ordering work against the step. */
 void *sph_get_stream(sph_handle *h);

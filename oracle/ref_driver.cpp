@@ -24,7 +24,12 @@
 
 extern "C" {
 
-void *ref_create(void) { return new SPHSystem(); }
+void *ref_create(void)
+{
+    cudaSetDevice(0);
+    cudaFree(0);   /* create the context before the constructor's allocations */
+    return new SPHSystem();
+}
 
 int ref_dim(void) { return REF_DIM; }
 
@@ -122,10 +127,31 @@ void ref_set_use_cylinder(void *h, int on)
 }
 #endif
 
-/* One reference step, then a device synchronise so errors surface here. */
+/* One reference step, then a device synchronise so errors surface here.
+ * Before stepping, the reference's own set_parameters() is called once and
+ * its status checked: if the parameter block does not reach the device
+ * (see ref_shim/cutil_math.h), the step would hash every particle to an
+ * out-of-range cell, so the driver refuses to run it and returns -1. */
 int ref_step(void *h)
 {
     SPHSystem *s = (SPHSystem *)h;
+    /* every particle inside the box: its hash indexes the cell arrays */
+    for (uint i = 0; i < s->m_num_particle; ++i) {
+        const Particle &p = s->m_host_mem[i];
+#if REF_DIM == 2
+        if (!(p.pos.x >= 0.0f && p.pos.x < s->m_world_width && p.pos.y >= 0.0f && p.pos.y < s->m_world_depth))
+            return -2;
+#else
+        if (!(p.pos.x >= 0.0f && p.pos.x < s->m_world_width && p.pos.y >= 0.0f && p.pos.y < s->m_world_height &&
+              p.pos.z >= 0.0f && p.pos.z < s->m_world_length))
+            return -2;
+#endif
+        if (p.level != 1 && p.level != 2) return -3;
+    }
+    cudaGetLastError();
+    s->m_host_param->num_particle = s->m_num_particle;
+    set_parameters(s->m_host_param);
+    if (cudaGetLastError() != cudaSuccess) return -1;
     s->m_sys_running = 1;
 #if REF_DIM == 2
     s->animate();

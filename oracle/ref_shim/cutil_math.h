@@ -15,6 +15,22 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+/*
+ * The reference uploads its parameter block with
+ *     cudaMemcpyToSymbol((char *)&dev_param, host_param, sizeof(SysParam));
+ * (SPH-3D-2/sph_system.cu:36).  Under the CUDA 3/4 runtime it was written
+ * for, a char* argument was the symbol address itself.  Under CUDA 12 that
+ * call binds to the template overload, which takes the address of the
+ * temporary pointer instead, fails with an invalid-symbol error and leaves
+ * dev_param zeroed (cell_size 0 -> every hash saturates -> out-of-bounds
+ * cell writes).  This exact-match overload restores the old meaning so the
+ * unmodified source uploads its constants.
+ */
+static inline cudaError_t cudaMemcpyToSymbol(char *symbol, const void *src, size_t count)
+{
+    return ::cudaMemcpyToSymbol((const void *)symbol, src, count, 0, cudaMemcpyHostToDevice);
+}
+
 #define SHIM_HD __host__ __device__ inline
 
 SHIM_HD float2 make_float2(float s) { return make_float2(s, s); }

@@ -49,6 +49,19 @@ def _u(a):
 STATE_FIELDS = ("pos", "vel", "ev", "acc", "dens", "press", "energy", "surface", "level", "interior")
 
 
+def particle_dtype(dim):
+    """numpy dtype of the reference's Particle record (SPH-3D-2/sph_system.h:8-24,
+    SPH-2D/sph_system.h:7-22)."""
+    if dim == 3:
+        return np.dtype({"names": ["pos", "vel", "ev", "acc", "dens", "press", "energy", "surface", "tension",
+                                   "level"],
+                         "formats": [("<f4", 3)] * 4 + ["<f4"] * 5 + ["<u4"],
+                         "offsets": [0, 12, 24, 36, 48, 52, 56, 60, 64, 68], "itemsize": 72})
+    return np.dtype({"names": ["pos", "vel", "ev", "acc", "dens", "press", "energy", "level", "surface"],
+                     "formats": [("<f4", 2)] * 4 + ["<f4"] * 3 + ["<u4", "<f4"],
+                     "offsets": [0, 8, 16, 24, 32, 36, 40, 44, 48], "itemsize": 56})
+
+
 class Solver:
     """One solver instance on the current CUDA device."""
 
@@ -155,6 +168,40 @@ class Solver:
         out["trans_vel"] = arr["trans_vel"][: n * self.dim].reshape(n, self.dim).copy()
         out["n"] = n
         return out
+
+    # -- reference-layout records (SPHSystem::m_host_mem) ------------------
+    @property
+    def record_size(self):
+        return int(self._lib.sph_particle_record_size(self._h))
+
+    def read_particles_into(self, host_ptr, capacity_bytes):
+        """Copies the state as reference Particle records to host memory at
+        host_ptr (ideally page-locked); returns the record count."""
+        n = C.c_uint32()
+        self._check(self._lib.sph_read_particles(self._h, C.c_void_p(host_ptr), int(capacity_bytes), C.byref(n)),
+                    "sph_read_particles")
+        return int(n.value)
+
+    def write_particles_from(self, host_ptr, n):
+        self._check(self._lib.sph_write_particles(self._h, C.c_void_p(host_ptr), int(n)), "sph_write_particles")
+
+    def read_particles(self):
+        """Reference-layout records as a numpy structured array."""
+        n = self.num_particles()
+        buf = np.zeros(max(n, 1) * self.record_size, np.uint8)
+        got = self.read_particles_into(buf.ctypes.data, buf.nbytes)
+        return buf[: got * self.record_size].view(particle_dtype(self.dim))
+
+    # -- profiling ---------------------------------------------------------
+    def set_profiling(self, on=True):
+        self._check(self._lib.sph_set_profiling(self._h, 1 if on else 0), "sph_set_profiling")
+
+    def stage_times(self):
+        ms = (C.c_float * 32)()
+        names = (C.c_char_p * 32)()
+        cnt = C.c_int()
+        self._check(self._lib.sph_stage_times(self._h, ms, names, 32, C.byref(cnt)), "sph_stage_times")
+        return [(names[k].decode(), float(ms[k])) for k in range(min(cnt.value, 32))]
 
     # -- stepping ----------------------------------------------------------
     def step(self, nsteps=1):

@@ -109,6 +109,11 @@ SIGNATURES = [
     ("sph_get_num_particles", C.c_int, [H, UP]),
     ("sph_get_state", C.c_int, [H, C.POINTER(StateView)]),
     ("sph_get_debug", C.c_int, [H, C.POINTER(DebugView)]),
+    ("sph_particle_record_size", C.c_uint32, [H]),
+    ("sph_read_particles", C.c_int, [H, C.c_void_p, C.c_uint64, UP]),
+    ("sph_write_particles", C.c_int, [H, C.c_void_p, C.c_uint32]),
+    ("sph_set_profiling", C.c_int, [H, C.c_int]),
+    ("sph_stage_times", C.c_int, [H, FP, C.POINTER(C.c_char_p), C.c_int, C.POINTER(C.c_int)]),
     ("sph_get_stream", C.c_void_p, [H]),
     ("sph_set_debug", C.c_int, [H, C.c_int]),
     ("sph_last_launch_count", C.c_int, [H, UP]),

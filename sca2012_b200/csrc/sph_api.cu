@@ -43,6 +43,14 @@ struct sph_handle {
     // density grid + marching cubes
     McBuffers mc;
     bool grid_valid = false;
+    // reference-layout staging buffer (allocated on first use)
+    float *aos = nullptr;
+    // per-stage profiling
+    static constexpr int kMaxStages = 24;
+    bool profiling = false;
+    cudaEvent_t ev[kMaxStages + 1] = {};
+    const char *stage_name[kMaxStages] = {};
+    int nstages = 0;
 };
 
 namespace {
@@ -111,6 +119,14 @@ void scan_u32(sph_handle *h, const uint32_t *in, uint32_t *out, const uint32_t *
     h->last_launches += 3;
 }
 
+// Records the end of a named stage when profiling (event 0 marks the start).
+void stage(sph_handle *h, const char *name)
+{
+    if (!h->profiling || h->nstages >= sph_handle::kMaxStages) return;
+    h->stage_name[h->nstages] = name;
+    cudaEventRecord(h->ev[++h->nstages], h->stream);
+}
+
 template <int DIM> int run_step(sph_handle *h)
 {
     const sph_config &c = h->cfg;
@@ -119,30 +135,41 @@ template <int DIM> int run_step(sph_handle *h)
     CanonPtrs in = h->buf[p], out = h->buf[p ^ 1];
     WorkPtrs w = h->w;
     const uint32_t G = grid_for(h, h->n_ub);
-    const uint32_t GC = grid_for(h, h->ncells);
     cudaStream_t s = h->stream;
+    h->nstages = 0;
+    if (h->profiling) cudaEventRecord(h->ev[0], s);
 
     cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, s);
     k_hash<DIM><<<G, kThreads, 0, s>>>(c, cin, in, w);
+    stage(h, "hash");
     scan_u32(h, w.cell_count, w.cell_off, nullptr, h->ncells, h->scan_grand, 1, nullptr);
+    stage(h, "scan_cells");
     k_scatter<<<G, kThreads, 0, s>>>(cin, w);
+    stage(h, "scatter");
     k_reorder<<<G, kThreads, 0, s>>>(cin, in, w);
+    stage(h, "reorder");
     k_density<DIM><<<G, kThreads, 0, s>>>(c, cin, w);
+    stage(h, "density");
     k_force_integrate<DIM><<<G, kThreads, 0, s>>>(c, cin, w);
+    stage(h, "force_integrate");
     k_energy_split<DIM><<<G, kThreads, 0, s>>>(c, cin, in, w, h->debug ? 1 : 0);
-    h->last_launches += 7;
+    stage(h, "energy_split");
+    h->last_launches += 6;
     scan_u32(h, w.split_c, w.split_rank, &cin->n, 0, &cin->n_split, 0, w.split_list);
     k_split_guard<<<1, 1, 0, s>>>(c, cin, h->cap);
     h->last_launches += 1;
+    stage(h, "scan_split");
     if (c.use_merge) {
         const uint32_t GM = grid_for(h, (uint32_t)std::min<uint64_t>((uint64_t)h->ncells * 32u, 1u << 30));
         k_merge<DIM><<<GM, kThreads, 0, s>>>(c, cin, in, w, h->ncells, h->cap);
         h->last_launches += 1;
+        stage(h, "merge");
     }
     scan_u32(h, w.removed_c, w.removed_rank, &cin->n, 0, &cin->n_removed, 0, nullptr);
+    stage(h, "scan_removed");
     k_write<DIM><<<G, kThreads, 0, s>>>(c, cin, cout, out, w);
     h->last_launches += 1;
-    (void)GC;
+    stage(h, "write");
     h->cur = p ^ 1;
     uint64_t ub = h->n_ub;
     if (c.use_split) ub *= (c.split_ways == 4 ? 4u : 2u);
@@ -261,6 +288,8 @@ int sph_destroy(sph_handle *h)
 {
     if (!h) return SPH_ERR_INVALID;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    for (int k = 0; k <= sph_handle::kMaxStages; ++k)
+        if (h->ev[k]) cudaEventDestroy(h->ev[k]);
     for (void *p : h->allocs) cudaFree(p);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -476,6 +505,80 @@ int sph_get_debug(sph_handle *h, sph_debug_view *d)
     }
     if (d->removed) cudaMemcpy(d->removed, w.removed_c, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
     return cuda_check(h, "sph_get_debug");
+}
+
+uint32_t sph_particle_record_size(const sph_handle *h)
+{
+    if (!h) return 0;
+    return h->cfg.dim == 3 ? 4u * AosLayout<3>::words : 4u * AosLayout<2>::words;
+}
+
+static int ensure_aos(sph_handle *h)
+{
+    if (h->aos) return SPH_OK;
+    return dalloc(h, &h->aos, (size_t)h->cap * AosLayout<3>::words);
+}
+
+int sph_read_particles(sph_handle *h, void *host_dst, uint64_t capacity_bytes, uint32_t *n_out)
+{
+    if (!h || !n_out) return SPH_ERR_INVALID;
+    if (int rc = ensure_aos(h)) return rc;
+    const uint32_t n = read_n(h);
+    const uint64_t rec = sph_particle_record_size(h);
+    *n_out = n;
+    if (!host_dst) return SPH_OK;
+    if (capacity_bytes < rec * n) { h->err = "sph_read_particles: destination too small"; return SPH_ERR_INVALID; }
+    const uint32_t G = grid_for(h, n);
+    if (h->cfg.dim == 3) k_to_aos<3><<<G, kThreads, 0, h->stream>>>(h->cnt + h->cur, h->buf[h->cur], h->aos);
+    else k_to_aos<2><<<G, kThreads, 0, h->stream>>>(h->cnt + h->cur, h->buf[h->cur], h->aos);
+    cudaMemcpyAsync(host_dst, h->aos, rec * n, cudaMemcpyDeviceToHost, h->stream);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) { h->err = cudaGetErrorString(e); return SPH_ERR_CUDA; }
+    return cuda_check(h, "sph_read_particles");
+}
+
+int sph_write_particles(sph_handle *h, const void *host_src, uint32_t n)
+{
+    if (!h || (n && !host_src)) return SPH_ERR_INVALID;
+    if (n > h->cap) { h->err = "sph_write_particles: capacity exceeded"; return SPH_ERR_CAPACITY; }
+    if (int rc = ensure_aos(h)) return rc;
+    const uint64_t rec = sph_particle_record_size(h);
+    cudaMemcpyAsync(h->aos, host_src, rec * n, cudaMemcpyHostToDevice, h->stream);
+    const uint32_t G = grid_for(h, n);
+    if (h->cfg.dim == 3) k_from_aos<3><<<G, kThreads, 0, h->stream>>>(n, h->buf[h->cur], h->aos);
+    else k_from_aos<2><<<G, kThreads, 0, h->stream>>>(n, h->buf[h->cur], h->aos);
+    // the count goes through a tiny kernel-free copy on the same stream
+    static thread_local uint32_t n_host;
+    n_host = n;
+    cudaMemcpyAsync(&h->cnt[h->cur].n, &n_host, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream);
+    cudaStreamSynchronize(h->stream);
+    h->n_ub = n;
+    h->have_step = false;
+    return cuda_check(h, "sph_write_particles");
+}
+
+int sph_set_profiling(sph_handle *h, int on)
+{
+    if (!h) return SPH_ERR_INVALID;
+    if (on && !h->ev[0])
+        for (int k = 0; k <= sph_handle::kMaxStages; ++k) cudaEventCreate(&h->ev[k]);
+    h->profiling = on != 0;
+    return cuda_check(h, "sph_set_profiling");
+}
+
+int sph_stage_times(sph_handle *h, float *ms, const char **names, int max, int *count)
+{
+    if (!h || !count) return SPH_ERR_INVALID;
+    if (!h->profiling) { h->err = "profiling is off"; return SPH_ERR_INVALID; }
+    cudaStreamSynchronize(h->stream);
+    *count = h->nstages;
+    for (int k = 0; k < h->nstages && k < max; ++k) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, h->ev[k], h->ev[k + 1]);
+        if (ms) ms[k] = t;
+        if (names) names[k] = h->stage_name[k];
+    }
+    return cuda_check(h, "sph_stage_times");
 }
 
 void *sph_get_stream(sph_handle *h) { return h ? (void *)h->stream : nullptr; }

@@ -670,6 +670,59 @@ __global__ void __launch_bounds__(kThreads) k_write(sph_config c, const Counters
     }
 }
 
+// ------------------------------------------------------------ reference-layout records
+// 3D Particle (SPH-3D-2/sph_system.h:8-24), 18 words:
+//   pos3 vel3 ev3 acc3 dens press energy surface tension level(u32)
+// 2D Particle (SPH-2D/sph_system.h:7-22), 14 words (56 B, 8-byte aligned):
+//   pos2 vel2 ev2 acc2 dens pres energy level(u32) surface_normal pad
+template <int DIM> struct AosLayout;
+template <> struct AosLayout<3> { static constexpr int words = 18; };
+template <> struct AosLayout<2> { static constexpr int words = 14; };
+
+template <int DIM>
+__global__ void __launch_bounds__(kThreads) k_to_aos(const Counters *__restrict__ cnt, CanonPtrs st, float *aos)
+{
+    const uint32_t n = cnt->n;
+    constexpr int W = AosLayout<DIM>::words;
+    for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) {
+        const float4 p = st.pos[i], v = st.vel[i], e = st.ev[i], a = st.acc[i];
+        float *o = aos + (size_t)i * W;
+        if (DIM == 3) {
+            o[0] = p.x; o[1] = p.y; o[2] = p.z; o[3] = v.x; o[4] = v.y; o[5] = v.z;
+            o[6] = e.x; o[7] = e.y; o[8] = e.z; o[9] = a.x; o[10] = a.y; o[11] = a.z;
+            o[12] = st.dens[i]; o[13] = st.press[i]; o[14] = st.energy[i]; o[15] = st.surface[i];
+            o[16] = 0.0f; o[17] = __uint_as_float((uint32_t)p.w);
+        } else {
+            o[0] = p.x; o[1] = p.y; o[2] = v.x; o[3] = v.y; o[4] = e.x; o[5] = e.y; o[6] = a.x; o[7] = a.y;
+            o[8] = st.dens[i]; o[9] = st.press[i]; o[10] = st.energy[i];
+            o[11] = __uint_as_float((uint32_t)p.w); o[12] = st.surface[i]; o[13] = 0.0f;
+        }
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kThreads) k_from_aos(uint32_t n, CanonPtrs st, const float *aos)
+{
+    constexpr int W = AosLayout<DIM>::words;
+    for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) {
+        const float *o = aos + (size_t)i * W;
+        if (DIM == 3) {
+            st.pos[i] = make_float4(o[0], o[1], o[2], (float)__float_as_uint(o[17]));
+            st.vel[i] = make_float4(o[3], o[4], o[5], 0.f);
+            st.ev[i] = make_float4(o[6], o[7], o[8], 0.f);
+            st.acc[i] = make_float4(o[9], o[10], o[11], 0.f);
+            st.dens[i] = o[12]; st.press[i] = o[13]; st.energy[i] = o[14]; st.surface[i] = o[15];
+        } else {
+            st.pos[i] = make_float4(o[0], o[1], 0.f, (float)__float_as_uint(o[11]));
+            st.vel[i] = make_float4(o[2], o[3], 0.f, 0.f);
+            st.ev[i] = make_float4(o[4], o[5], 0.f, 0.f);
+            st.acc[i] = make_float4(o[6], o[7], 0.f, 0.f);
+            st.dens[i] = o[8]; st.press[i] = o[9]; st.energy[i] = o[10]; st.surface[i] = o[12];
+        }
+        st.interior[i] = 0u;
+    }
+}
+
 // ------------------------------------------------------------ debug helpers
 __global__ void k_cell_ranges(const uint32_t *__restrict__ off, uint32_t ncells, uint32_t *start, uint32_t *end)
 {

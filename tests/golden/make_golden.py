@@ -26,7 +26,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 REF = os.path.join(ROOT, "oracle", "_ref")
 
 # variant: (dim, warm-up steps, crop x below this value or None)
-VARIANTS = {"2d": (2, 10, None), "3d2": (3, 8, None), "3d4": (3, 4, 14.0)}
+VARIANTS = {"2d": (2, 10, None), "3d2": (3, 8, 6.0), "3d4": (3, 4, 10.0)}
 
 
 def particle_dtype(dim, size):
@@ -89,6 +89,10 @@ def read_debug(lib, h, n, dim, ncell):
 
 def step_checked(lib, h):
     rc = lib.ref_step(h)
+    if rc == -1:
+        raise RuntimeError("reference parameter upload failed; step not run")
+    if rc in (-2, -3):
+        raise RuntimeError("state outside the box or with an unknown level; step not run")
     if rc != 0:
         raise RuntimeError(f"reference step reported CUDA error {rc}")
 
@@ -99,6 +103,32 @@ def check_state(buf, dim, world):
         raise RuntimeError("non-finite position in the reference state; stopping before the next step")
     if (p < 0).any() or (p > np.asarray(world[:dim])).any():
         raise RuntimeError("position outside the box; stopping before the next step")
+
+
+def mesh_digest(mesh):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(mesh, np.float32).tobytes()).hexdigest()
+
+
+def compact(out):
+    """Fixture layout: the density grid and its normals sparse (non-zero
+    nodes only), the marching-cubes mesh as its triangle count and SHA-256
+    (the reference's own CPU marching cubes, oracle/_ref/libref_*_mc.so,
+    must reproduce it from the grid), and no copy of the grid-step state
+    (identical to s1_off: same input, split/merge off)."""
+    res = {k: v for k, v in out.items() if k not in ("grid_dens", "grid_normal", "mesh", "s1_grid", "init")}
+    if "grid_dens" in out:
+        d, nrm = out["grid_dens"], out["grid_normal"]
+        if not np.array_equal(out["s1_grid"].view(np.uint8), out["s1_off"].view(np.uint8)):
+            raise RuntimeError("grid step state differs from the split/merge-off step state")
+        nz = np.flatnonzero(d).astype(np.uint32)
+        res["grid_dens_idx"], res["grid_dens_val"] = nz, d[nz]
+        nn = np.flatnonzero(np.any(nrm != 0, axis=1)).astype(np.uint32)
+        res["grid_normal_idx"], res["grid_normal_val"] = nn, nrm[nn]
+        res["grid_nodes"] = np.uint32(len(d))
+        res["mesh_triangles"] = np.uint32(len(out["mesh"]))
+        res["mesh_sha256"] = np.array(mesh_digest(out["mesh"]))
+    return res
 
 
 def run_variant(v, out_dir):
@@ -114,10 +144,8 @@ def run_variant(v, out_dir):
     ncell = lib.ref_total_cell(h)
 
     lib.ref_add_default_scene(h, 0)
-    init = read_state_host = None
     n0 = lib.ref_num_particles(h)
-    # the host copy holds the scene after add_*; read it through the device
-    # round trip (one step would change it), so re-upload it as the state
+    # the host copy holds the scene add_*() built; re-upload it (cropped) as the state
     init = np.zeros(n0, dt)
     lib.ref_read_particles(h, ptr(init))
     if crop is not None:
@@ -158,7 +186,7 @@ def run_variant(v, out_dir):
         out["mesh"] = np.stack([t[:nt] for t in tri], 1)   # nt x 6 x 3 (v0 v1 v2 n0 n1 n2)
         out["s1_grid"] = read_state(lib, h, dt)
     path = os.path.join(out_dir, f"ref_{v}.npz")
-    np.savez_compressed(path, **out)
+    np.savez_compressed(path, **compact(out))
     print(f"{v}: n={n} -> off {len(out['s1_off'])}, on {len(out['s1_on'])}; wrote {path} "
           f"({os.path.getsize(path) / 1e6:.2f} MB)")
 
@@ -166,8 +194,16 @@ def run_variant(v, out_dir):
 def main():
     out_dir = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden")
     os.makedirs(out_dir, exist_ok=True)
+    only = sys.argv[2] if len(sys.argv) > 2 else None
+    if only:
+        run_variant(only, out_dir)
+        return
+    # one process per variant: each reference build carries its own runtime
+    import subprocess
+    rc = 0
     for v in VARIANTS:
-        run_variant(v, out_dir)
+        rc |= subprocess.run([sys.executable, os.path.abspath(__file__), out_dir, v]).returncode
+    sys.exit(rc)
 
 
 if __name__ == "__main__":

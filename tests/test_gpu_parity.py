@@ -31,20 +31,19 @@ def _crop(scene, xmax):
     return pos[m], vel[m], lvl[m]
 
 
-def _cfg(preset, split, merge):
+def _cfg(preset, split, merge, n):
     c = sph.preset(preset)
     c.use_split = int(split)
     c.use_merge = int(merge)
-    if c.max_particle > 2_000_000:
-        c.max_particle = 2_000_000
+    c.max_particle = max(4 * n * (c.split_ways - 1) + n, 1024)
     return c
 
 
 def run_case(name):
     preset, scene, warm = CASES[name]
-    cfg_on = _cfg(preset, 1, 1)
-    cfg_off = _cfg(preset, 0, 0)
-    pos, vel, lvl = scene(cfg_on)
+    pos, vel, lvl = scene(sph.preset(preset))
+    cfg_on = _cfg(preset, 1, 1, len(pos))
+    cfg_off = _cfg(preset, 0, 0, len(pos))
     s = sph.Solver(cfg_on)
     s.set_debug(True)
     s.set_state(dict(pos=pos, vel=vel, level=lvl))
