@@ -137,6 +137,10 @@ typedef struct sph_config {
     uint32_t ndens[3];
     float iso_value;
     uint32_t mc_interpolate; /* 0: edge midpoints (reference); 1: linear interpolation */
+    uint32_t splat_with_kernel; /* 0: grid splat radius = particle radius (reference); 1: kernel length */
+    uint32_t grid_every;     /* density grid + surface inside every k-th step (0: never); the
+                                reference's display mode 2 is 1 (SPH-3D-2/sph_system.cpp:336-362) */
+    uint32_t max_triangles;  /* device mesh capacity (0: 3 per grid node) */
 } sph_config;
 
 /* Host view of a particle state (SoA).  Vectors hold `dim` floats per
@@ -239,9 +243,17 @@ int sph_last_launch_count(const sph_handle *h, uint32_t *launches);
  * to host arrays of ndens[0]*ndens[1]*ndens[2] floats / 3*that floats. */
 int sph_density_grid(sph_handle *h, float *dens, float *normal);
 
-/* Density grid + marching cubes on the device; triangles appended in the
- * reference's cell order (x outer, y, z inner). */
+/* Triangles of the surface extracted on the device by the last step that
+ * built the density grid (grid_every), appended in the reference's cell
+ * order (x outer, y, z inner; SPH-3D-2/sph_system.cpp:517-542).  Returns
+ * SPH_ERR_CAPACITY if the surface had more triangles than the capacities
+ * (max_triangles of the config or of the mesh view): the mesh then holds the
+ * first triangles and num_triangles the full count. */
 int sph_extract_surface(sph_handle *h, sph_mesh_view *mesh);
+
+/* Marching cubes on the device over a caller-supplied grid (host arrays in
+ * sph_density_grid's layout), with sph_extract_surface's output. */
+int sph_surface_from_grid(sph_handle *h, const float *dens, const float *normal, sph_mesh_view *mesh);
 
 /* Human-readable text of the last error on this handle (static storage). */
 const char *sph_last_error(const sph_handle *h);

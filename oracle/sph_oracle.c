@@ -760,13 +760,16 @@ void oracle_density_grid(const sph_config *c, uint32_t n, const float *pos, cons
                 uint32_t j = index[s];
                 const int lj = lv(level[j]);
                 const float *pj = pos + (size_t)j * 3;
-                float rad2 = c->radius[lj] * c->radius[lj];
+                /* particle radius (reference) or kernel length (splat_with_kernel) */
+                float rad = c->splat_with_kernel ? c->kernel[lj] : c->radius[lj];
+                float rad2 = rad * rad;
                 float r2f = r2_f32(c, pj, np);
                 if (r2f < rad2) {                        /* :1894-1900 */
                     double r2 = 0.0;
                     for (int a = 0; a < 3; ++a) { double q = (double)pj[a] - (double)np[a]; r2 += q * q; }
                     double t = (double)rad2 - r2;
-                    acc_ += (double)c->mass[lj] * (double)c->poly6_radius[lj] * t * t * t;
+                    double w = c->splat_with_kernel ? (double)c->poly6[lj] : (double)c->poly6_radius[lj];
+                    acc_ += (double)c->mass[lj] * w * t * t * t;
                 }
             }
         }

@@ -62,7 +62,8 @@ class Config(C.Structure):
         ("extern_force_on", C.c_uint32), ("extern_click", F2), ("extern_force", F2),
         ("extern_len", C.c_float), ("extern_coe", C.c_float),
         ("dens_mul", C.c_uint32), ("den_size", C.c_float), ("ndens", U3), ("iso_value", C.c_float),
-        ("mc_interpolate", C.c_uint32),
+        ("mc_interpolate", C.c_uint32), ("splat_with_kernel", C.c_uint32), ("grid_every", C.c_uint32),
+        ("max_triangles", C.c_uint32),
     ]
 
     def copy(self):
@@ -119,8 +120,10 @@ SIGNATURES = [
     ("sph_last_launch_count", C.c_int, [H, UP]),
     ("sph_density_grid", C.c_int, [H, FP, FP]),
     ("sph_extract_surface", C.c_int, [H, C.POINTER(MeshView)]),
+    ("sph_surface_from_grid", C.c_int, [H, FP, FP, C.POINTER(MeshView)]),
     ("sph_last_error", C.c_char_p, [H]),
 ]
+
 
 LIB_NAME = "libsca2012_b200.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)

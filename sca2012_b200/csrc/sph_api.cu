@@ -43,6 +43,7 @@ struct sph_handle {
     // density grid + marching cubes
     McBuffers mc;
     bool grid_valid = false;
+    uint64_t step_index = 0;
     // reference-layout staging buffer (allocated on first use)
     float *aos = nullptr;
     // per-stage profiling
@@ -119,6 +120,18 @@ void scan_u32(sph_handle *h, const uint32_t *in, uint32_t *out, const uint32_t *
     h->last_launches += 3;
 }
 
+// Marching cubes over the current device grid: classify, scan, emit.
+void run_mc(sph_handle *h)
+{
+    McBuffers &mc = h->mc;
+    const uint32_t GQ = grid_for(h, mc.cubes);
+    k_mc_count<<<GQ, kThreads, 0, h->stream>>>(h->cfg, mc.dens, mc.cube_cnt);
+    scan_u32(h, mc.cube_cnt, mc.cube_off, nullptr, mc.cubes, mc.num_tri, 0, nullptr);
+    k_mc_emit<<<GQ, kThreads, 0, h->stream>>>(h->cfg, mc.dens, mc.normal, mc.cube_cnt, mc.cube_off, mc.max_tri,
+                                               mc.tri);
+    h->last_launches += 2;
+}
+
 // Records the end of a named stage when profiling (event 0 marks the start).
 void stage(sph_handle *h, const char *name)
 {
@@ -152,6 +165,16 @@ template <int DIM> int run_step(sph_handle *h)
     stage(h, "density");
     k_force_integrate<DIM><<<G, kThreads, 0, s>>>(c, cin, w);
     stage(h, "force_integrate");
+    // density grid + surface mid-step: stale cell lists, integrated positions
+    // (SPH-3D-2/sph_system.cpp:336-362)
+    if (DIM == 3 && c.grid_every && h->mc.nodes && h->step_index % c.grid_every == 0) {
+        k_splat<<<grid_for(h, h->mc.nodes), kThreads, 0, s>>>(c, w.cell_off, w.spos_n, h->mc.dens);
+        k_grid_normals<<<grid_for(h, h->mc.nodes), kThreads, 0, s>>>(c, h->mc.dens, h->mc.normal);
+        h->last_launches += 2;
+        run_mc(h);
+        h->grid_valid = true;
+        stage(h, "surface");
+    }
     k_energy_split<DIM><<<G, kThreads, 0, s>>>(c, cin, in, w, h->debug ? 1 : 0);
     stage(h, "energy_split");
     h->last_launches += 6;
@@ -171,6 +194,7 @@ template <int DIM> int run_step(sph_handle *h)
     h->last_launches += 1;
     stage(h, "write");
     h->cur = p ^ 1;
+    h->step_index++;
     uint64_t ub = h->n_ub;
     if (c.use_split) ub *= (c.split_ways == 4 ? 4u : 2u);
     h->n_ub = (uint32_t)std::min<uint64_t>(ub, h->cap);
@@ -606,17 +630,65 @@ extern "C" {
 int sph_density_grid(sph_handle *h, float *dens, float *normal)
 {
     if (!h) return SPH_ERR_INVALID;
-    (void)dens; (void)normal;
-    h->err = "sph_density_grid: not available in this build";
-    return SPH_ERR_INVALID;
+    if (!h->mc.nodes) { h->err = "no density grid (2D, or ndens unset)"; return SPH_ERR_INVALID; }
+    if (!h->grid_valid) { h->err = "no grid yet: set grid_every and step"; return SPH_ERR_INVALID; }
+    cudaStreamSynchronize(h->stream);
+    const uint32_t G = h->mc.nodes;
+    if (dens) cudaMemcpy(dens, h->mc.dens, sizeof(float) * G, cudaMemcpyDeviceToHost);
+    if (normal) {
+        std::vector<float4> t(G);
+        cudaMemcpy(t.data(), h->mc.normal, sizeof(float4) * G, cudaMemcpyDeviceToHost);
+        for (uint32_t g = 0; g < G; ++g) {
+            normal[3 * (size_t)g] = t[g].x;
+            normal[3 * (size_t)g + 1] = t[g].y;
+            normal[3 * (size_t)g + 2] = t[g].z;
+        }
+    }
+    return cuda_check(h, "sph_density_grid");
+}
+
+static int copy_mesh(sph_handle *h, sph_mesh_view *mesh)
+{
+    cudaStreamSynchronize(h->stream);
+    uint32_t total = 0;
+    cudaMemcpy(&total, h->mc.num_tri, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    mesh->num_triangles = total;
+    const uint32_t on_dev = std::min(total, h->mc.max_tri);
+    const uint32_t nt = std::min(on_dev, mesh->max_triangles);
+    float *dst[6] = {mesh->v0, mesh->v1, mesh->v2, mesh->n0, mesh->n1, mesh->n2};
+    for (int k = 0; k < 6; ++k)
+        if (dst[k] && nt)
+            cudaMemcpy(dst[k], h->mc.tri + 3ull * h->mc.max_tri * k, sizeof(float) * 3ull * nt,
+                       cudaMemcpyDeviceToHost);
+    if (int rc = cuda_check(h, "surface copy")) return rc;
+    if (total > h->mc.max_tri || total > mesh->max_triangles) {
+        h->err = "surface has more triangles than the mesh capacity (truncated)";
+        return SPH_ERR_CAPACITY;
+    }
+    return SPH_OK;
 }
 
 int sph_extract_surface(sph_handle *h, sph_mesh_view *mesh)
 {
-    if (!h) return SPH_ERR_INVALID;
-    (void)mesh;
-    h->err = "sph_extract_surface: not available in this build";
-    return SPH_ERR_INVALID;
+    if (!h || !mesh) return SPH_ERR_INVALID;
+    if (!h->mc.nodes) { h->err = "no density grid (2D, or ndens unset)"; return SPH_ERR_INVALID; }
+    if (!h->grid_valid) { h->err = "no surface yet: set grid_every and step"; return SPH_ERR_INVALID; }
+    return copy_mesh(h, mesh);
+}
+
+int sph_surface_from_grid(sph_handle *h, const float *dens, const float *normal, sph_mesh_view *mesh)
+{
+    if (!h || !dens || !normal || !mesh) return SPH_ERR_INVALID;
+    if (!h->mc.nodes) { h->err = "no density grid (2D, or ndens unset)"; return SPH_ERR_INVALID; }
+    const uint32_t G = h->mc.nodes;
+    std::vector<float4> t(G);
+    for (uint32_t g = 0; g < G; ++g)
+        t[g] = make_float4(normal[3 * (size_t)g], normal[3 * (size_t)g + 1], normal[3 * (size_t)g + 2], 0.f);
+    cudaMemcpyAsync(h->mc.dens, dens, sizeof(float) * G, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->mc.normal, t.data(), sizeof(float4) * G, cudaMemcpyHostToDevice, h->stream);
+    run_mc(h);
+    h->grid_valid = true;
+    return copy_mesh(h, mesh);
 }
 
 }  // extern "C"

@@ -240,8 +240,10 @@ void preset_si(sph_config *c, int dim, float s, uint32_t ways, float dt)
     c->split_density_ratio = 0.9f;
     c->merge_interior_steps = 50;
     c->split_copies_fields = 1;
-    c->iso_value = 0.5f * 1000.0f;
+    c->iso_value = 0.5f * 1000.0f;   // iso-level 0.5 * rest density
     c->mc_interpolate = 1;
+    c->splat_with_kernel = 1;        // grid density ~ SPH density, so the iso value means 0.5 rho0
+    c->max_triangles = 2000000;
 }
 
 }  // namespace
@@ -282,7 +284,8 @@ extern "C" int sph_config_preset(int preset, sph_config *c)
         c->max_particle = 1114112u * 4u;
         c->use_split = 1;
         c->use_merge = 1;
-        set_mc_grid(c, 2);
+        set_mc_grid(c, 2);   // 257 x 257 x 129 nodes at 0.005
+        c->grid_every = 10;  // marching cubes every 10 steps
         return SPH_OK;
     case SPH_PRESET_ROLLOUT_3D:
         // 32^3 block at s = 0.01 in 0.64^3, two-way

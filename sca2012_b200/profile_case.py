@@ -1,0 +1,46 @@
+"""Fixed workload runner for profiling the step's kernels under ncu.
+
+    python -m sca2012_b200.profile_case [--particles N] [--steps K] [--adaptive 0|1]
+
+Runs the four-way dam-break workload (the bench workload, optionally with the
+block shrunk to about N particles) for K steps on cuda:0 and exits 0.  Every
+step issues each kernel once, so `ncu -k regex:<kernel> -s <K-1> -c 1`
+captures the last step's launch.  Device memory stays near 450 bytes per
+particle of capacity (capacity = 1.5 x the initial count).
+"""
+import argparse
+import sys
+
+import numpy as np
+
+import sca2012_b200 as sph
+from sca2012_b200 import scenes
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--particles", type=int, default=0, help="0 = full 1,114,112-particle workload")
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--adaptive", type=int, default=1)
+    a = ap.parse_args()
+    cfg = sph.preset(sph.PRESET_DAM_3D4)
+    pos, vel, lvl = scenes.dam_3d4(cfg)
+    if a.particles and a.particles < len(pos):
+        keep = np.argsort(pos[:, 0], kind="stable")[: a.particles]
+        keep.sort()
+        pos, vel, lvl = pos[keep], vel[keep], lvl[keep]
+    cfg.use_split = a.adaptive
+    cfg.use_merge = a.adaptive
+    cfg.max_particle = int(len(pos) * 1.5) + 1024
+    s = sph.Solver(cfg)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    s.step(a.steps)
+    rc = s.sync_status()
+    n = s.num_particles()
+    s.close()
+    print(f"profile_case: {len(pos)} -> {n} particles after {a.steps} steps, status {rc}")
+    return 0 if rc == 0 else 1
+
+
+if __name__ == "__main__":
+    sys.exit(main())
