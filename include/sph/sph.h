@@ -255,6 +255,28 @@ int sph_extract_surface(sph_handle *h, sph_mesh_view *mesh);
  * sph_density_grid's layout), with sph_extract_surface's output. */
 int sph_surface_from_grid(sph_handle *h, const float *dens, const float *normal, sph_mesh_view *mesh);
 
+/*
+ * Cell sort that allocates nothing.  No counterpart in the reference (its
+ * cell sort is calc_hash + thrust::sort_by_key + find_start_end, which
+ * allocate; see sph_step).  For callers that cannot call cudaMalloc — a host
+ * program whose device memory belongs to another allocator, or a loop that
+ * cannot afford cudaMalloc's implicit device synchronisation.  Sorts n
+ * particles (pos_dev: n*dim floats on the device) by cell key exactly like
+ * sph_step does and writes, all on the device, key_dev[n] and index_dev[n]
+ * (cell key and particle index of each sorted slot) and cell_start_dev /
+ * cell_end_dev (one entry per cell; 0xffffffff / 0 for an empty cell).
+ * Scratch lives in one fixed static device array: at most
+ * SPH_NOALLOC_MAX_PARTICLES particles and SPH_NOALLOC_MAX_CELLS cells, larger
+ * inputs return SPH_ERR_RANGE.  The first call on a device looks up the
+ * array's device address; make it before any stream capture begins.  Calls
+ * share the array, so calls that overlap on the GPU race.  Asynchronous on
+ * `stream` (a cudaStream_t, NULL = default stream).
+ */
+#define SPH_NOALLOC_MAX_PARTICLES (1u << 18)
+#define SPH_NOALLOC_MAX_CELLS (1u << 16)
+int sph_sort_cells_noalloc(const sph_config *cfg, uint32_t n, const float *pos_dev, uint32_t *key_dev,
+                           uint32_t *index_dev, uint32_t *cell_start_dev, uint32_t *cell_end_dev, void *stream);
+
 /* Human-readable text of the last error on this handle (static storage). */
 const char *sph_last_error(const sph_handle *h);
 

@@ -122,8 +122,12 @@ SIGNATURES = [
     ("sph_extract_surface", C.c_int, [H, C.POINTER(MeshView)]),
     ("sph_surface_from_grid", C.c_int, [H, FP, FP, C.POINTER(MeshView)]),
     ("sph_last_error", C.c_char_p, [H]),
+    ("sph_sort_cells_noalloc", C.c_int, [C.POINTER(Config), C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.c_void_p]),
 ]
 
+NOALLOC_MAX_PARTICLES = 1 << 18
+NOALLOC_MAX_CELLS = 1 << 16
 
 LIB_NAME = "libsca2012_b200.so"
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
