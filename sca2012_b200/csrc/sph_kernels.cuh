@@ -194,25 +194,31 @@ __global__ void __launch_bounds__(kThreads) k_density(sph_config c, const Counte
         q.z = DIM == 3 ? k / (c.ncell[0] * c.ncell[1]) : 0u;
         float rho = 0.0f;
         uint32_t nb = 0;
+        const float m0 = c.mass[0], m1 = c.mass[1], skip = c.density_skip_r2;
+        auto add = [&](uint32_t t, float4 pj) {
+            float dx, dyy, dzz;
+            const float r2 = r2_of<DIM>(pj, pi, dx, dyy, dzz);
+            if (t != s && !(r2 < skip) && r2 < h2) {
+                const float x = h2 - r2;
+                rho += (pj.w == 1.0f ? m0 : m1) * poly6 * (x * x * x);
+                ++nb;
+            }
+        };
 #pragma unroll 1
         for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
 #pragma unroll 1
             for (int dy = -1; dy <= 1; ++dy) {
                 uint32_t b, e;
                 if (!row_range<DIM>(c, w.cell_off, q, dy, dz, b, e)) continue;
-                for (uint32_t t = b; t < e; ++t) {
-                    const float4 pj = w.spos[t];
-                    if (t == s) continue;
-                    float dx, dyy, dzz;
-                    float r2 = r2_of<DIM>(pj, pi, dx, dyy, dzz);
-                    if (r2 < c.density_skip_r2) continue;
-                    if (r2 < h2) {
-                        float x = h2 - r2;
-                        float mj = pj.w == 1.0f ? c.mass[0] : c.mass[1];
-                        rho += mj * poly6 * (x * x * x);
-                        ++nb;
-                    }
+                uint32_t t = b;
+                for (; t + 4 <= e; t += 4) {
+                    const float4 p0 = w.spos[t], p1 = w.spos[t + 1], p2 = w.spos[t + 2], p3 = w.spos[t + 3];
+                    add(t, p0);
+                    add(t + 1, p1);
+                    add(t + 2, p2);
+                    add(t + 3, p3);
                 }
+                for (; t < e; ++t) add(t, w.spos[t]);
             }
         rho += c.mass[li] * poly6 * c.kernel6[li];   // self term
         float r = rho / c.rest_density;
@@ -227,10 +233,20 @@ __global__ void __launch_bounds__(kThreads) k_density(sph_config c, const Counte
 // 2D SPH-2D/sph_system.cu:462-790), then the integrator and walls
 // (SPH-3D-2/sph_system.cu:204-322, SPH-2D/sph_system.cu:198-252).  The
 // integrated state goes to the *_n arrays so the loop never sees it.
+// Neighbour loops run in two phases: phase A streams a row's candidates with
+// the cheap FP32 r^2 test (independent loads, unrolled) and appends the
+// in-range slots to a per-thread list in shared memory (interleaved, so the
+// 32 lanes of a warp hit 32 banks); phase B runs the interaction math only
+// over that list.  Without it every candidate paid the predicated
+// interaction math.  A full list is drained early, so any neighbour count
+// works.
+constexpr uint32_t kListLen = 48;   // 48 x 256 x 4 B = 48 KB of shared memory per block
+
 template <int DIM>
 __global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, const Counters *__restrict__ cnt,
                                                               WorkPtrs w)
 {
+    __shared__ uint32_t nlist[kListLen][kThreads];
     const uint32_t n = cnt->n;
     for (uint32_t s = grid_stride_start(); s < n; s += grid_stride()) {
         const float4 pi = w.spos[s];
@@ -249,26 +265,21 @@ __global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, cons
         q.y = (k / c.ncell[0]) % c.ncell[1];
         q.z = DIM == 3 ? k / (c.ncell[0] * c.ncell[1]) : 0u;
         float fx = 0.f, fy = 0.f, fz = 0.f, gx = 0.f, gy = 0.f, gz = 0.f, lap = 0.f;
-#pragma unroll 1
-        for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
-#pragma unroll 1
-            for (int dy = -1; dy <= 1; ++dy) {
-                uint32_t b, e;
-                if (!row_range<DIM>(c, w.cell_off, q, dy, dz, b, e)) continue;
-                for (uint32_t t = b; t < e; ++t) {
-                    const float4 pj = w.spos[t];
-                    if (t == s) {
-                        if (DIM == 2)   // SPH-2D/sph_system.cu:599-603 (0 with the integer 3/4)
-                            lap += ilap * ai.w * hi2 * (0.0f - c.lapc_three_quarters * hi2);
-                        continue;
-                    }
-                    float rx, ry, rz;
-                    float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
-                    const int lj = lv(pj.w);
-                    const float maxh2 = fmaxf(hi2, c.kernel2[lj]);
-                    if (!(r2 < maxh2)) continue;
-                    if (r2 < 0.0001f) continue;
-                    const float r = __fsqrt_rn(r2);
+        if (DIM == 2)   // self term, SPH-2D/sph_system.cu:599-603 (0 with the integer 3/4)
+            lap += ilap * ai.w * hi2 * (0.0f - c.lapc_three_quarters * hi2);
+        // pairs with r^2 < max(h_i^2, h_j^2) and r^2 >= 1e-4 (:797-804)
+        const float cut0 = fmaxf(hi2, c.kernel2[0]), cut1 = fmaxf(hi2, c.kernel2[1]);
+        uint32_t *my_list = &nlist[0][threadIdx.x];
+        uint32_t cntl = 0;
+        // phase B: the interaction math over the listed neighbours
+        auto flush = [&]() {
+            for (uint32_t kk = 0; kk < cntl; ++kk) {
+                const uint32_t t = my_list[kk * kThreads];
+                const float4 pj = w.spos[t];
+                float rx, ry, rz;
+                const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
+                const int lj = lv(pj.w);
+                const float r = __fsqrt_rn(r2);
                     const float4 aj = w.saux[t];
                     const float4 evj = w.sev[t];
                     float ipk = 0.f, ivk = 0.f, jpk = 0.f, jvk = 0.f;
@@ -294,8 +305,36 @@ __global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, cons
                     fx += -rx * tp + (evj.x - evi.x) * tv;
                     fy += -ry * tp + (evj.y - evi.y) * tv;
                     if (DIM == 3) fz += -rz * tp + (evj.z - evi.z) * tv;
-                }
             }
+            cntl = 0;
+        };
+        // phase A: stream the candidates, keep the ones within reach
+        auto consider = [&](uint32_t t, float4 pj) {
+            float rx, ry, rz;
+            const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
+            const float cut = pj.w == 1.0f ? cut0 : cut1;
+            if (t != s && r2 < cut && !(r2 < 0.0001f)) {
+                my_list[cntl * kThreads] = t;
+                if (++cntl == kListLen) flush();
+            }
+        };
+#pragma unroll 1
+        for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy) {
+                uint32_t b, e;
+                if (!row_range<DIM>(c, w.cell_off, q, dy, dz, b, e)) continue;
+                uint32_t t = b;
+                for (; t + 4 <= e; t += 4) {
+                    const float4 p0 = w.spos[t], p1 = w.spos[t + 1], p2 = w.spos[t + 2], p3 = w.spos[t + 3];
+                    consider(t, p0);
+                    consider(t + 1, p1);
+                    consider(t + 2, p2);
+                    consider(t + 3, p3);
+                }
+                for (; t < e; ++t) consider(t, w.spos[t]);
+            }
+        flush();
         // surface tension switch (SPH-3D-2/sph_system.cu:1113-1136)
         const float nrm = sqrtf(gx * gx + gy * gy + gz * gz);
         if (nrm > c.surface_threshold) {
@@ -394,6 +433,7 @@ template <int DIM>
 __global__ void __launch_bounds__(kThreads) k_energy_split(sph_config c, Counters *__restrict__ cnt,
                                                            CanonPtrs st, WorkPtrs w, int want_tv)
 {
+    __shared__ uint32_t nlist[kListLen][kThreads];
     const uint32_t n = cnt->n;
     // 2/(PI^0.25 * sqrt(3 sigma)) with PI = 3.141592f, sigma = 2
     const float amp = 2.0f / (powf(3.141592f, 0.25f) * sqrtf(6.0f));
@@ -405,30 +445,54 @@ __global__ void __launch_bounds__(kThreads) k_energy_split(sph_config c, Counter
         const float ih = 1.0f / h, isq = 1.0f / sqrtf(h);
         const uint3 q = cell_of<DIM>(c, pi);
         float tsx = 0.f, tsy = 0.f, tsz = 0.f, tvx = 0.f, tvy = 0.f, tvz = 0.f;
+        const float skip = c.energy_skip_close ? 0.0001f : 0.0f;   // :1229-1232 (2D keeps close pairs)
+        uint32_t *my_list = &nlist[0][threadIdx.x];
+        uint32_t cntl = 0;
+        // phase B: the wavelet transform over the listed neighbours
+        auto flush = [&]() {
+            for (uint32_t kk = 0; kk < cntl; ++kk) {
+                const uint32_t t = my_list[kk * kThreads];
+                const float4 pj = w.spos_n[t];
+                const float4 vj = w.svel_n[t];
+                float rx, ry, rz;
+                r2_of<DIM>(pi, pj, rx, ry, rz);
+                const float wx = wavelet(rx * ih, amp), wy = wavelet(ry * ih, amp);
+                tsx += wx; tsy += wy;
+                tvx += vj.x * wx * isq; tvy += vj.y * wy * isq;
+                if (DIM == 3) {
+                    const float wz = wavelet(rz * ih, amp);
+                    tsz += wz;
+                    tvz += vj.z * wz * isq;
+                }
+            }
+            cntl = 0;
+        };
+        // phase A: j != i with skip <= r^2 < h^2 (:1222-1233)
+        auto consider = [&](uint32_t t, float4 pj) {
+            float rx, ry, rz;
+            const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
+            if (t != s && r2 < h2 && !(r2 < skip)) {
+                my_list[cntl * kThreads] = t;
+                if (++cntl == kListLen) flush();
+            }
+        };
 #pragma unroll 1
         for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
 #pragma unroll 1
             for (int dy = -1; dy <= 1; ++dy) {
                 uint32_t b, e;
                 if (!row_range<DIM>(c, w.cell_off, q, dy, dz, b, e)) continue;
-                for (uint32_t t = b; t < e; ++t) {
-                    if (t == s) continue;
-                    const float4 pj = w.spos_n[t];
-                    float rx, ry, rz;
-                    float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
-                    if (!(r2 < h2)) continue;
-                    if (c.energy_skip_close && r2 < 0.0001f) continue;
-                    const float4 vj = w.svel_n[t];
-                    float wx = wavelet(rx * ih, amp), wy = wavelet(ry * ih, amp);
-                    tsx += wx; tsy += wy;
-                    tvx += vj.x * wx * isq; tvy += vj.y * wy * isq;
-                    if (DIM == 3) {
-                        float wz = wavelet(rz * ih, amp);
-                        tsz += wz;
-                        tvz += vj.z * wz * isq;
-                    }
+                uint32_t t = b;
+                for (; t + 4 <= e; t += 4) {
+                    const float4 p0 = w.spos_n[t], p1 = w.spos_n[t + 1], p2 = w.spos_n[t + 2], p3 = w.spos_n[t + 3];
+                    consider(t, p0);
+                    consider(t + 1, p1);
+                    consider(t + 2, p2);
+                    consider(t + 3, p3);
                 }
+                for (; t < e; ++t) consider(t, w.spos_n[t]);
             }
+        flush();
         tvx /= tsx; tvy /= tsy; tvz = DIM == 3 ? tvz / tsz : 0.f;
         float energy = 0.5f * (tvx * tvx + tvy * tvy);
         if (c.energy_mass_weight) energy *= c.mass[li];
