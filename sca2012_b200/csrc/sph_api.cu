@@ -183,7 +183,7 @@ template <int DIM> int run_step(sph_handle *h)
     h->last_launches += 1;
     stage(h, "scan_split");
     if (c.use_merge) {
-        const uint32_t GM = grid_for(h, (uint32_t)std::min<uint64_t>((uint64_t)h->ncells * 32u, 1u << 30));
+        const uint32_t GM = grid_for(h, h->ncells);   // a warp scans 32 cells at a time
         k_merge<DIM><<<GM, kThreads, 0, s>>>(c, cin, in, w, h->ncells, h->cap);
         h->last_launches += 1;
         stage(h, "merge");

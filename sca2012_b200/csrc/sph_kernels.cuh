@@ -127,6 +127,31 @@ __device__ __forceinline__ int row_range(const sph_config &c, const uint32_t *__
     return 1;
 }
 
+// As row_range, for FRESH cell lists (every member lies inside its cell):
+// drops the row when the slab it spans in y/z is farther from p than the
+// cut-off, and the row's end cells when they are.  A cell is dropped only if
+// its distance exceeds sqrt(cut2 * 1.001), far above the FP32 rounding of
+// the positions, so every pair the exact r^2 test accepts stays in range.
+template <int DIM>
+__device__ __forceinline__ int row_range_pruned(const sph_config &c, const uint32_t *__restrict__ off, uint3 q,
+                                                float4 p, float cut2, int dy, int dz, uint32_t &b, uint32_t &e)
+{
+    int y = (int)q.y + dy, z = (int)q.z + dz;
+    if (y < 0 || y >= (int)c.ncell[1]) return 0;
+    if (DIM == 3 && (z < 0 || z >= (int)c.ncell[2])) return 0;
+    const float cs = c.cell_size, lim = cut2 * 1.001f;
+    const float ey = dy < 0 ? p.y - (float)q.y * cs : (dy > 0 ? (float)(q.y + 1) * cs - p.y : 0.0f);
+    const float ez = DIM == 3 ? (dz < 0 ? p.z - (float)q.z * cs : (dz > 0 ? (float)(q.z + 1) * cs - p.z : 0.0f)) : 0.0f;
+    const float base = fmaxf(ey, 0.0f) * fmaxf(ey, 0.0f) + fmaxf(ez, 0.0f) * fmaxf(ez, 0.0f);
+    if (!(base < lim)) return 0;
+    const float ex0 = fmaxf(p.x - (float)q.x * cs, 0.0f), ex1 = fmaxf((float)(q.x + 1) * cs - p.x, 0.0f);
+    const uint32_t x0 = (q.x > 0 && ex0 * ex0 + base < lim) ? q.x - 1 : q.x;
+    const uint32_t x1 = (q.x + 1 < c.ncell[0] && ex1 * ex1 + base < lim) ? q.x + 1 : q.x;
+    b = __ldg(off + key_of(c, x0, (uint32_t)y, (uint32_t)z));
+    e = __ldg(off + key_of(c, x1, (uint32_t)y, (uint32_t)z) + 1);
+    return 1;
+}
+
 // ------------------------------------------------------------ 1. hash
 template <int DIM>
 __global__ void __launch_bounds__(kThreads) k_hash(sph_config c, const Counters *__restrict__ cnt,
@@ -173,6 +198,15 @@ __global__ void __launch_bounds__(kThreads) k_reorder(const Counters *__restrict
     }
 }
 
+// Neighbour loops run in two phases: phase A streams a row's candidates with
+// the cheap FP32 r^2 test (independent loads, unrolled) and appends the
+// in-range slots to a per-thread list in shared memory (interleaved, so the
+// 32 lanes of a warp hit 32 banks); phase B runs the interaction math only
+// over that list.  Without it every candidate paid the predicated
+// interaction math.  A full list is drained early, so any neighbour count
+// works.
+constexpr uint32_t kListLen = 48;   // 48 x 256 x 4 B = 48 KB of shared memory per block
+
 // ------------------------------------------------------------ 5. density
 // rho_i = m_i poly6_i h_i^6 + sum_{j != i, skip <= r^2 < h_i^2} m_j poly6_i (h_i^2 - r^2)^3
 // p_i = k ((rho_i / rho0)^3 - 1)         (SPH-3D-2/sph_system.cu:338-677)
@@ -180,8 +214,6 @@ template <int DIM>
 __global__ void __launch_bounds__(kThreads) k_density(sph_config c, const Counters *__restrict__ cnt, WorkPtrs w)
 {
     const uint32_t n = cnt->n;
-    const float *off_unused = nullptr;
-    (void)off_unused;
     for (uint32_t s = grid_stride_start(); s < n; s += grid_stride()) {
         const float4 pi = w.spos[s];
         const int li = lv(pi.w);
@@ -195,6 +227,8 @@ __global__ void __launch_bounds__(kThreads) k_density(sph_config c, const Counte
         float rho = 0.0f;
         uint32_t nb = 0;
         const float m0 = c.mass[0], m1 = c.mass[1], skip = c.density_skip_r2;
+        // single pass: the kernel sum is cheap enough to run predicated
+        // (:394-417, j != i with skip <= r^2 < h_i^2)
         auto add = [&](uint32_t t, float4 pj) {
             float dx, dyy, dzz;
             const float r2 = r2_of<DIM>(pj, pi, dx, dyy, dzz);
@@ -209,7 +243,7 @@ __global__ void __launch_bounds__(kThreads) k_density(sph_config c, const Counte
 #pragma unroll 1
             for (int dy = -1; dy <= 1; ++dy) {
                 uint32_t b, e;
-                if (!row_range<DIM>(c, w.cell_off, q, dy, dz, b, e)) continue;
+                if (!row_range_pruned<DIM>(c, w.cell_off, q, pi, h2, dy, dz, b, e)) continue;
                 uint32_t t = b;
                 for (; t + 4 <= e; t += 4) {
                     const float4 p0 = w.spos[t], p1 = w.spos[t + 1], p2 = w.spos[t + 2], p3 = w.spos[t + 3];
@@ -233,15 +267,6 @@ __global__ void __launch_bounds__(kThreads) k_density(sph_config c, const Counte
 // 2D SPH-2D/sph_system.cu:462-790), then the integrator and walls
 // (SPH-3D-2/sph_system.cu:204-322, SPH-2D/sph_system.cu:198-252).  The
 // integrated state goes to the *_n arrays so the loop never sees it.
-// Neighbour loops run in two phases: phase A streams a row's candidates with
-// the cheap FP32 r^2 test (independent loads, unrolled) and appends the
-// in-range slots to a per-thread list in shared memory (interleaved, so the
-// 32 lanes of a warp hit 32 banks); phase B runs the interaction math only
-// over that list.  Without it every candidate paid the predicated
-// interaction math.  A full list is drained early, so any neighbour count
-// works.
-constexpr uint32_t kListLen = 48;   // 48 x 256 x 4 B = 48 KB of shared memory per block
-
 template <int DIM>
 __global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, const Counters *__restrict__ cnt,
                                                               WorkPtrs w)
@@ -609,9 +634,17 @@ __global__ void __launch_bounds__(kThreads) k_merge(sph_config c, const Counters
     const uint32_t ways = c.split_ways == 4 ? 4u : 2u;
     const uint32_t extra = ways - 1u;
     const float hs2 = c.kernel[1] / 2.0f;
-    for (uint32_t cell = blockIdx.x * (blockDim.x >> 5) + wib; cell < ncells; cell += warps_total) {
+    // each warp takes 32 consecutive cells at a time: one lane per cell reads
+    // its member count, and the warp then works only on the cells that hold
+    // enough members to form a group
+    for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + wib) * 32u; base < ncells; base += warps_total * 32u) {
+        const uint32_t mine = base + lane;
+        const uint32_t members = mine < ncells ? w.cell_off[mine + 1] - w.cell_off[mine] : 0u;
+        uint32_t todo = __ballot_sync(0xffffffffu, members >= ways);
+        while (todo) {
+        const uint32_t cell = base + (__ffs(todo) - 1);
+        todo &= todo - 1;
         const uint32_t b = w.cell_off[cell], e = w.cell_off[cell + 1];
-        if (e - b < ways) continue;
         // 2D rule: the criterion of the particle whose INDEX equals the cell
         // index, as memory holds it at merge time (SPH-2D/sph_system.cu:1207)
         float cell_score = 0.f;
@@ -660,6 +693,7 @@ __global__ void __launch_bounds__(kThreads) k_merge(sph_config c, const Counters
             }
         }
         __syncwarp();
+        }
     }
 }
 
@@ -688,8 +722,10 @@ __global__ void __launch_bounds__(kThreads) k_write(sph_config c, const Counters
         cnt_next->n_removed = 0;
         cnt_next->split_off = 0;
     }
-    for (uint32_t s = grid_stride_start(); s < n; s += grid_stride()) {
-        const uint32_t i = w.sidx[s];
+    // one thread per particle index: reads gather from the sorted slot, the
+    // writes (survivors keep their order) stay coalesced
+    for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) {
+        const uint32_t s = w.inv[i];
         const uint32_t sp = split_on & w.split_c[i];
         const uint32_t rm = w.removed_c[i];
         const uint32_t rr = w.removed_rank[i];
