@@ -279,6 +279,30 @@ def run_ours(args, rank, world, local_rank):
     status |= s.sync_status()
     s.close()
 
+    # --- the reference's own default 3D-2 scene (7,220 particles, split and
+    # merge on): launch-bound, so eager launches vs CUDA-graph replay
+    from sca2012_b200 import scenes as _sc
+    small = {}
+    rcfg = sph.preset(sph.PRESET_REF_3D2)
+    rcfg.use_split = rcfg.use_merge = 1
+    rpos, rvel, rlvl = _sc.ref_box_3d2(rcfg)
+    for mode in ("eager", "graph"):
+        rs = sph.Solver(rcfg)
+        rs.set_graph(mode == "graph")
+        rs.set_state(dict(pos=rpos, vel=rvel, level=rlvl))
+        rs.step(5)
+        rst = torch.cuda.ExternalStream(rs.stream_ptr)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(rst)
+        rs.step(50)
+        b.record(rst)
+        b.synchronize()
+        small[mode + "_ms_per_step"] = a.elapsed_time(b) / 50
+        status |= rs.sync_status()
+        rs.close()
+    small["particles_initial"] = len(rpos)
+
     out = None
     if rank == 0:
         cpu = None
@@ -306,6 +330,7 @@ def run_ours(args, rank, world, local_rank):
                          "launch_ms": stage_avg[top], "peak_source": peak_src,
                          "note": "neighbour loops are FP32-issue bound: the HBM fraction is low by design"},
             "stages_ms": stage_avg,
+            "ref_3d2_default_scene": small,
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": launches,

@@ -202,6 +202,12 @@ int sph_set_state(sph_handle *h, const sph_state_view *st);
 /* Advances nsteps steps on the handle's stream (asynchronous). */
 int sph_step(sph_handle *h, int nsteps);
 
+/* on != 0: sph_step replays each step as a CUDA graph (one per buffer
+ * parity, recaptured when the config or the launch grid changes); steps that
+ * build the density grid and surface run uncaptured.  Same results, fewer
+ * launch overheads for small particle counts. */
+int sph_set_graph(sph_handle *h, int on);
+
 /* Synchronises and returns the device-side status (capacity / non-finite). */
 int sph_sync(sph_handle *h);
 

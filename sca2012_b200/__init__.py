@@ -100,6 +100,10 @@ class Solver:
     def set_debug(self, on=True):
         self._check(self._lib.sph_set_debug(self._h, 1 if on else 0), "sph_set_debug")
 
+    def set_graph(self, on=True):
+        """Replay steps as captured CUDA graphs (same results, fewer launches)."""
+        self._check(self._lib.sph_set_graph(self._h, 1 if on else 0), "sph_set_graph")
+
     @property
     def stream_ptr(self):
         return self._lib.sph_get_stream(self._h)

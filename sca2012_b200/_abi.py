@@ -106,6 +106,7 @@ SIGNATURES = [
     ("sph_add_particles", C.c_int, [H, C.c_uint32, FP, FP, UP]),
     ("sph_set_state", C.c_int, [H, C.POINTER(StateView)]),
     ("sph_step", C.c_int, [H, C.c_int]),
+    ("sph_set_graph", C.c_int, [H, C.c_int]),
     ("sph_sync", C.c_int, [H]),
     ("sph_get_num_particles", C.c_int, [H, UP]),
     ("sph_get_state", C.c_int, [H, C.POINTER(StateView)]),

@@ -52,6 +52,11 @@ struct sph_handle {
     cudaEvent_t ev[kMaxStages + 1] = {};
     const char *stage_name[kMaxStages] = {};
     int nstages = 0;
+    // CUDA graphs of one step, one per buffer parity
+    bool use_graph = false;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    uint32_t graph_grid[2] = {0, 0};
+    uint32_t graph_launches[2] = {0, 0};
 };
 
 namespace {
@@ -314,6 +319,8 @@ int sph_destroy(sph_handle *h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (int k = 0; k <= sph_handle::kMaxStages; ++k)
         if (h->ev[k]) cudaEventDestroy(h->ev[k]);
+    for (int p = 0; p < 2; ++p)
+        if (h->graph[p]) cudaGraphExecDestroy(h->graph[p]);
     for (void *p : h->allocs) cudaFree(p);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -335,6 +342,11 @@ int sph_set_config(sph_handle *h, const sph_config *cfg)
         return SPH_ERR_INVALID;
     }
     h->cfg = *cfg;
+    // captured steps hold the old constants as kernel arguments
+    for (int p = 0; p < 2; ++p) {
+        if (h->graph[p]) cudaGraphExecDestroy(h->graph[p]);
+        h->graph[p] = nullptr;
+    }
     return SPH_OK;
 }
 
@@ -408,6 +420,44 @@ int sph_set_state(sph_handle *h, const sph_state_view *st)
     return cuda_check(h, "sph_set_state");
 }
 
+static void drop_graphs(sph_handle *h)
+{
+    for (int p = 0; p < 2; ++p) {
+        if (h->graph[p]) cudaGraphExecDestroy(h->graph[p]);
+        h->graph[p] = nullptr;
+        h->graph_grid[p] = 0;
+    }
+}
+
+// Records one step for the current parity into a graph (nothing executes
+// during capture), restoring the host-side bookkeeping the recording moved.
+static int capture_step(sph_handle *h)
+{
+    const int p = h->cur;
+    const uint64_t step_index = h->step_index;
+    const uint32_t n_ub = h->n_ub, launches = h->last_launches;
+    cudaGraph_t g = nullptr;
+    h->last_launches = 0;
+    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return cuda_check(h, "cudaStreamBeginCapture");
+    int rc = h->cfg.dim == 3 ? run_step<3>(h) : run_step<2>(h);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    h->graph_launches[p] = h->last_launches;
+    h->cur = p;
+    h->step_index = step_index;
+    h->n_ub = n_ub;
+    h->last_launches = launches;
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_check(h, "cudaStreamEndCapture");
+    if (h->graph[p]) cudaGraphExecDestroy(h->graph[p]);
+    h->graph[p] = nullptr;
+    e = cudaGraphInstantiate(&h->graph[p], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_check(h, "cudaGraphInstantiate");
+    h->graph_grid[p] = grid_for(h, h->n_ub);
+    return SPH_OK;
+}
+
 int sph_step(sph_handle *h, int nsteps)
 {
     if (!h || nsteps < 0) return SPH_ERR_INVALID;
@@ -415,10 +465,38 @@ int sph_step(sph_handle *h, int nsteps)
     for (int k = 0; k < nsteps; ++k) {
         if (h->n_ub == 0) break;
         h->n_last_sorted = 0;   // resolved lazily by sph_get_debug
-        int rc = h->cfg.dim == 3 ? run_step<3>(h) : run_step<2>(h);
+        const bool surface_due = h->cfg.dim == 3 && h->cfg.grid_every && h->mc.nodes &&
+                                 h->step_index % h->cfg.grid_every == 0;
+        int rc;
+        if (h->use_graph && !h->profiling && !surface_due) {
+            const int p = h->cur;
+            if (!h->graph[p] || h->graph_grid[p] != grid_for(h, h->n_ub)) {
+                rc = capture_step(h);
+                if (rc) return rc;
+            }
+            if (cudaGraphLaunch(h->graph[p], h->stream) != cudaSuccess) return cuda_check(h, "cudaGraphLaunch");
+            // the bookkeeping run_step does on the host
+            h->cur = p ^ 1;
+            h->step_index++;
+            uint64_t ub = h->n_ub;
+            if (h->cfg.use_split) ub *= (h->cfg.split_ways == 4 ? 4u : 2u);
+            h->n_ub = (uint32_t)std::min<uint64_t>(ub, h->cap);
+            h->last_launches += h->graph_launches[p];
+            rc = SPH_OK;
+        } else {
+            rc = h->cfg.dim == 3 ? run_step<3>(h) : run_step<2>(h);
+        }
         if (rc) return rc;
         h->have_step = true;
     }
+    return SPH_OK;
+}
+
+int sph_set_graph(sph_handle *h, int on)
+{
+    if (!h) return SPH_ERR_INVALID;
+    h->use_graph = on != 0;
+    if (!h->use_graph) drop_graphs(h);
     return SPH_OK;
 }
 
@@ -618,6 +696,10 @@ int sph_set_debug(sph_handle *h, int on)
 {
     if (!h) return SPH_ERR_INVALID;
     h->debug = on != 0;
+    for (int p = 0; p < 2; ++p) {   // the flag is a captured kernel argument
+        if (h->graph[p]) cudaGraphExecDestroy(h->graph[p]);
+        h->graph[p] = nullptr;
+    }
     return SPH_OK;
 }
 
