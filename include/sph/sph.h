@@ -261,6 +261,26 @@ int sph_extract_surface(sph_handle *h, sph_mesh_view *mesh);
  * sph_density_grid's layout), with sph_extract_surface's output. */
 int sph_surface_from_grid(sph_handle *h, const float *dens, const float *normal, sph_mesh_view *mesh);
 
+/* Headless POV-Ray scene files, replacing the reference app's make_mesh /
+ * make_particle (SPH-3D-2/sph_main.cpp:114-220): one smooth_triangle per mesh
+ * triangle, or one sphere per particle (red r 0.3 for level 1, yellow r 0.24
+ * for level 2); positions are p * scale + offset per axis (NULL: 1 and 0). */
+int sph_write_pov_mesh(const sph_mesh_view *mesh, const float *scale, const float *offset, const char *path);
+int sph_write_pov_particles(const float *pos, const uint32_t *level, uint32_t n, uint32_t dim, const float *scale,
+                            const float *offset, const char *path);
+
+/* Asynchronous readback: converts the current state to reference Particle
+ * records on a side stream, writing them and the record count straight into
+ * page-locked host memory that is mapped for the device (cudaHostAlloc with
+ * cudaHostAllocMapped, or cudaHostRegister with cudaHostRegisterMapped).
+ * Returns at once; the next sph_step overlaps the copy (it works on the other
+ * state buffer) and a later step that would overwrite the buffer being read
+ * waits for it.  sph_readback_wait blocks until the records and *count_dst
+ * are in host memory.  At most capacity_bytes are written (the count is still
+ * the full one). */
+int sph_read_particles_async(sph_handle *h, void *mapped_dst, uint64_t capacity_bytes, uint32_t *mapped_count_dst);
+int sph_readback_wait(sph_handle *h);
+
 /*
  * Cell sort that allocates nothing.  No counterpart in the reference (its
  * cell sort is calc_hash + thrust::sort_by_key + find_start_end, which

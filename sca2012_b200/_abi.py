@@ -122,6 +122,10 @@ SIGNATURES = [
     ("sph_density_grid", C.c_int, [H, FP, FP]),
     ("sph_extract_surface", C.c_int, [H, C.POINTER(MeshView)]),
     ("sph_surface_from_grid", C.c_int, [H, FP, FP, C.POINTER(MeshView)]),
+    ("sph_write_pov_mesh", C.c_int, [C.POINTER(MeshView), FP, FP, C.c_char_p]),
+    ("sph_write_pov_particles", C.c_int, [FP, UP, C.c_uint32, C.c_uint32, FP, FP, C.c_char_p]),
+    ("sph_read_particles_async", C.c_int, [H, C.c_void_p, C.c_uint64, C.c_void_p]),
+    ("sph_readback_wait", C.c_int, [H]),
     ("sph_last_error", C.c_char_p, [H]),
     ("sph_sort_cells_noalloc", C.c_int, [C.POINTER(Config), C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p]),

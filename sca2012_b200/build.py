@@ -15,7 +15,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsca2012_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["sph_api.cu", "sph_config.cpp", "sph_noalloc.cu"]
+SOURCES = ["sph_api.cu", "sph_config.cpp", "sph_noalloc.cu", "sph_pov.cpp"]
 
 
 def _newer(target, deps):

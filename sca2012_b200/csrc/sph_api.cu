@@ -52,6 +52,11 @@ struct sph_handle {
     cudaEvent_t ev[kMaxStages + 1] = {};
     const char *stage_name[kMaxStages] = {};
     int nstages = 0;
+    // asynchronous readback: side stream, per-parity completion events
+    cudaStream_t rb_stream = nullptr;
+    cudaEvent_t rb_ready = nullptr;
+    cudaEvent_t rb_done[2] = {nullptr, nullptr};
+    bool rb_pending[2] = {false, false};
     // CUDA graphs of one step, one per buffer parity
     bool use_graph = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -321,6 +326,13 @@ int sph_destroy(sph_handle *h)
         if (h->ev[k]) cudaEventDestroy(h->ev[k]);
     for (int p = 0; p < 2; ++p)
         if (h->graph[p]) cudaGraphExecDestroy(h->graph[p]);
+    if (h->rb_stream) {
+        cudaStreamSynchronize(h->rb_stream);
+        cudaStreamDestroy(h->rb_stream);
+        cudaEventDestroy(h->rb_ready);
+        cudaEventDestroy(h->rb_done[0]);
+        cudaEventDestroy(h->rb_done[1]);
+    }
     for (void *p : h->allocs) cudaFree(p);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -360,6 +372,7 @@ int sph_get_config(const sph_handle *h, sph_config *cfg)
 int sph_add_particles(sph_handle *h, uint32_t n, const float *pos, const float *vel, const uint32_t *level)
 {
     if (!h || (n && (!pos || !level))) return SPH_ERR_INVALID;
+    sph_readback_wait(h);   // the current buffer may still be read back
     const int dim = (int)h->cfg.dim;
     uint32_t n0 = read_n(h);
     if ((uint64_t)n0 + n > h->cap) { h->err = "sph_add_particles: capacity exceeded"; return SPH_ERR_CAPACITY; }
@@ -390,6 +403,7 @@ int sph_add_particles(sph_handle *h, uint32_t n, const float *pos, const float *
 int sph_set_state(sph_handle *h, const sph_state_view *st)
 {
     if (!h || !st) return SPH_ERR_INVALID;
+    sph_readback_wait(h);
     const uint32_t n = st->n;
     if (n > h->cap) { h->err = "sph_set_state: capacity exceeded"; return SPH_ERR_CAPACITY; }
     if (n && (!st->pos || !st->level)) return SPH_ERR_INVALID;
@@ -465,6 +479,11 @@ int sph_step(sph_handle *h, int nsteps)
     for (int k = 0; k < nsteps; ++k) {
         if (h->n_ub == 0) break;
         h->n_last_sorted = 0;   // resolved lazily by sph_get_debug
+        // this step writes the other state buffer: wait for a readback of it
+        if (h->rb_pending[h->cur ^ 1]) {
+            cudaStreamWaitEvent(h->stream, h->rb_done[h->cur ^ 1], 0);
+            h->rb_pending[h->cur ^ 1] = false;
+        }
         const bool surface_due = h->cfg.dim == 3 && h->cfg.grid_every && h->mc.nodes &&
                                  h->step_index % h->cfg.grid_every == 0;
         int rc;
@@ -643,6 +662,7 @@ int sph_write_particles(sph_handle *h, const void *host_src, uint32_t n)
 {
     if (!h || (n && !host_src)) return SPH_ERR_INVALID;
     if (n > h->cap) { h->err = "sph_write_particles: capacity exceeded"; return SPH_ERR_CAPACITY; }
+    sph_readback_wait(h);
     if (int rc = ensure_aos(h)) return rc;
     const uint64_t rec = sph_particle_record_size(h);
     cudaMemcpyAsync(h->aos, host_src, rec * n, cudaMemcpyHostToDevice, h->stream);
@@ -657,6 +677,47 @@ int sph_write_particles(sph_handle *h, const void *host_src, uint32_t n)
     h->n_ub = n;
     h->have_step = false;
     return cuda_check(h, "sph_write_particles");
+}
+
+int sph_read_particles_async(sph_handle *h, void *mapped_dst, uint64_t capacity_bytes, uint32_t *mapped_count_dst)
+{
+    if (!h || !mapped_dst || !mapped_count_dst) return SPH_ERR_INVALID;
+    void *dst_dev = nullptr, *cnt_dev = nullptr;
+    if (cudaHostGetDevicePointer(&dst_dev, mapped_dst, 0) != cudaSuccess ||
+        cudaHostGetDevicePointer(&cnt_dev, mapped_count_dst, 0) != cudaSuccess) {
+        cudaGetLastError();
+        h->err = "sph_read_particles_async: destination is not mapped page-locked memory";
+        return SPH_ERR_INVALID;
+    }
+    if (!h->rb_stream) {
+        if (cudaStreamCreateWithFlags(&h->rb_stream, cudaStreamNonBlocking) != cudaSuccess)
+            return cuda_check(h, "readback stream");
+        cudaEventCreateWithFlags(&h->rb_ready, cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&h->rb_done[0], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&h->rb_done[1], cudaEventDisableTiming);
+    }
+    const int p = h->cur;
+    const uint64_t rec = sph_particle_record_size(h);
+    const uint32_t max_rec = (uint32_t)std::min<uint64_t>(capacity_bytes / rec, h->cap);
+    cudaEventRecord(h->rb_ready, h->stream);
+    cudaStreamWaitEvent(h->rb_stream, h->rb_ready, 0);
+    const uint32_t G = grid_for(h, h->n_ub);
+    if (h->cfg.dim == 3)
+        k_to_aos_mapped<3><<<G, kThreads, 0, h->rb_stream>>>(h->cnt + p, h->buf[p], (float *)dst_dev, max_rec,
+                                                             (uint32_t *)cnt_dev);
+    else
+        k_to_aos_mapped<2><<<G, kThreads, 0, h->rb_stream>>>(h->cnt + p, h->buf[p], (float *)dst_dev, max_rec,
+                                                             (uint32_t *)cnt_dev);
+    cudaEventRecord(h->rb_done[p], h->rb_stream);
+    h->rb_pending[p] = true;
+    return cuda_check(h, "sph_read_particles_async");
+}
+
+int sph_readback_wait(sph_handle *h)
+{
+    if (!h) return SPH_ERR_INVALID;
+    if (h->rb_stream && cudaStreamSynchronize(h->rb_stream) != cudaSuccess) return cuda_check(h, "readback wait");
+    return SPH_OK;
 }
 
 int sph_set_profiling(sph_handle *h, int on)
