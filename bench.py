@@ -65,6 +65,8 @@ def parse():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--cpu-sample-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--batch-scenes", type=int, default=256, help="0 skips the batched-scenes comparison")
+    p.add_argument("--batch-steps", type=int, default=20)
     return p.parse_args()
 
 
@@ -303,6 +305,8 @@ def run_ours(args, rank, world, local_rank):
         rs.close()
     small["particles_initial"] = len(rpos)
 
+    batched = batched_scenes(args) if (world == 1 and args.batch_scenes) else None
+
     out = None
     if rank == 0:
         cpu = None
@@ -331,12 +335,94 @@ def run_ours(args, rank, world, local_rank):
                          "note": "neighbour loops are FP32-issue bound: the HBM fraction is low by design"},
             "stages_ms": stage_avg,
             "ref_3d2_default_scene": small,
+            "batched_scenes": batched,
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": launches,
             "status": status,
         }
     return out
+
+
+# ----------------------------------------------------------------- batched scenes
+def batched_scenes(args):
+    """256 independent dam-break scenes (128 2D, 128 3D two-way; sizes
+    log-uniform in [1024, 65536], per-scene viscosity and stiffness), split
+    and merge on.  Batched: one handle per dimensionality holding all its
+    scenes, each step replayed as a CUDA graph.  Baselines: one handle per
+    scene in its own box-sized world with plain (eager) launches, stepped
+    (a) one scene at a time, each synchronised before the next, and (b) all
+    handles' streams at once.  Scene-steps/s by wall clock around
+    synchronised loops (the baselines span 256 streams)."""
+    import torch
+    import sca2012_b200 as sph
+    from sca2012_b200 import scenes as sc
+    half = args.batch_scenes // 2
+    steps = args.batch_steps
+    batches = []
+    for pre, seed in ((sph.PRESET_DAM_2D, args.seed + 11), (sph.PRESET_DAM_3D2, args.seed + 12)):
+        base = sph.preset(pre)
+        base.use_split = base.use_merge = 1
+        batches.append(sc.batch_scenes(base, half, seed=seed))
+
+    def timed(solvers, k, per_scene_sync=False):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(k):
+            for h in solvers:
+                h.step(1)
+                if per_scene_sync:
+                    h.sync()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    # batched
+    bs = []
+    particles = 0
+    for cfg, boxes, pos, vel, lvl, scene, counts in batches:
+        h = sph.Solver(cfg)
+        h.set_scenes(boxes)
+        h.set_state(dict(pos=pos, vel=vel, level=lvl, scene=scene))
+        h.set_graph(True)
+        bs.append(h)
+        particles += len(pos)
+    timed(bs, 3)
+    t_batched = timed(bs, steps)
+    status = 0
+    for h in bs:
+        status |= h.sync_status()
+        h.close()
+    # one handle per scene
+    singles = []
+    for cfg, boxes, pos, vel, lvl, scene, counts in batches:
+        first = np.concatenate([[0], np.cumsum(counts)])
+        for k, (lo, hi, mu, stiff) in enumerate(boxes):
+            c1 = cfg.copy()
+            for a in range(int(cfg.dim)):
+                c1.ncell[a] = int(round((hi[a] - lo[a]) / float(cfg.cell_size)))
+                c1.world[a] = np.float32(c1.ncell[a]) * np.float32(cfg.cell_size)
+            c1.viscosity, c1.gas_constant = mu, stiff
+            c1.max_particle = int(4 * counts[k])
+            h = sph.Solver(c1)
+            sl = slice(first[k], first[k + 1])
+            h.set_state(dict(pos=pos[sl] - np.asarray(lo, np.float32), vel=vel[sl], level=lvl[sl]))
+            singles.append(h)
+    timed(singles, 2)
+    t_seq = timed(singles, steps, per_scene_sync=True)
+    t_conc = timed(singles, steps)
+    for h in singles:
+        status |= h.sync_status()
+        h.close()
+    n_sc = len(singles)
+    v_b = n_sc * steps / t_batched
+    v_s = n_sc * steps / t_seq
+    v_c = n_sc * steps / t_conc
+    return {"scenes": n_sc, "particles_initial": particles, "steps": steps,
+            "batched_scene_steps_per_s": v_b, "sequential_scene_steps_per_s": v_s,
+            "concurrent_streams_scene_steps_per_s": v_c,
+            "batched_vs_sequential": v_b / v_s, "batched_vs_concurrent_streams": v_b / v_c,
+            "batched_ms_per_step": t_batched / steps * 1e3, "status": status,
+            "timing": "wall clock around synchronised step loops"}
 
 
 # ----------------------------------------------------------------- reference arm

@@ -151,7 +151,19 @@ typedef struct sph_state_view {
     float *dens, *press, *energy, *surface;
     uint32_t *level;
     uint32_t *interior;      /* SPH_MERGE_INTERIOR counter */
+    uint32_t *scene;         /* scene index of each particle (batched scenes; 0 otherwise) */
 } sph_state_view;
+
+/* One scene of a batch: its walled box inside the handle's world and the
+ * constants that differ between scenes.  Boxes must be at least
+ * SPH_SCENE_GAP_CELLS cells apart so no particle pair across scenes is ever
+ * within a kernel length. */
+#define SPH_SCENE_GAP_CELLS 2
+typedef struct sph_scene {
+    float lo[3], hi[3];      /* walls: particles stay in [lo + r, hi - r] */
+    float viscosity;
+    float gas_constant;
+} sph_scene;
 
 /* Intermediates of the last step (host arrays sized by the caller).
  * n_sorted = particle count the step started with; total_cell = cells. */
@@ -201,6 +213,14 @@ int sph_set_state(sph_handle *h, const sph_state_view *st);
 
 /* Advances nsteps steps on the handle's stream (asynchronous). */
 int sph_step(sph_handle *h, int nsteps);
+
+/* Batched scenes: many independent scenes advance in the same launches.
+ * Each particle carries a scene index (sph_state_view.scene); scene s
+ * integrates inside scenes[s].lo/hi with its own viscosity and stiffness,
+ * all other constants are the handle's.  Every scene's particles evolve
+ * exactly as they would alone in a handle with the same world.  nscenes = 0
+ * returns to the single-scene box [0, world]. */
+int sph_set_scenes(sph_handle *h, uint32_t nscenes, const sph_scene *scenes);
 
 /* on != 0: sph_step replays each step as a CUDA graph (one per buffer
  * parity, recaptured when the config or the launch grid changes); steps that

@@ -46,7 +46,8 @@ def _u(a):
     return a.ctypes.data_as(_abi.UP) if a is not None else None
 
 
-STATE_FIELDS = ("pos", "vel", "ev", "acc", "dens", "press", "energy", "surface", "level", "interior")
+STATE_FIELDS = ("pos", "vel", "ev", "acc", "dens", "press", "energy", "surface", "level", "interior", "scene")
+_U32_FIELDS = ("level", "interior", "scene")
 
 
 def particle_dtype(dim):
@@ -104,6 +105,19 @@ class Solver:
         """Replay steps as captured CUDA graphs (same results, fewer launches)."""
         self._check(self._lib.sph_set_graph(self._h, 1 if on else 0), "sph_set_graph")
 
+    def set_scenes(self, boxes):
+        """Batched scenes: boxes is a list of (lo, hi, viscosity, gas_constant)
+        with lo/hi of length dim; a particle's `scene` state field indexes it.
+        An empty list returns to the single box [0, world]."""
+        arr = (_abi.Scene * max(1, len(boxes)))()
+        for s, (lo, hi, mu, k) in enumerate(boxes):
+            for d in range(self.dim):
+                arr[s].lo[d] = float(lo[d])
+                arr[s].hi[d] = float(hi[d])
+            arr[s].viscosity = float(mu)
+            arr[s].gas_constant = float(k)
+        self._check(self._lib.sph_set_scenes(self._h, len(boxes), arr), "sph_set_scenes")
+
     @property
     def stream_ptr(self):
         return self._lib.sph_get_stream(self._h)
@@ -127,9 +141,9 @@ class Solver:
             a = st.get(k)
             if a is None:
                 continue
-            a = np.ascontiguousarray(a, np.uint32 if k in ("level", "interior") else np.float32)
+            a = np.ascontiguousarray(a, np.uint32 if k in _U32_FIELDS else np.float32)
             keep[k] = a
-            setattr(v, k, _u(a) if k in ("level", "interior") else _f(a))
+            setattr(v, k, _u(a) if k in _U32_FIELDS else _f(a))
         self._check(self._lib.sph_set_state(self._h, C.byref(v)), "sph_set_state")
 
     def num_particles(self):
@@ -145,10 +159,11 @@ class Solver:
             out[k] = np.zeros(n, np.float32)
         out["level"] = np.zeros(n, np.uint32)
         out["interior"] = np.zeros(n, np.uint32)
+        out["scene"] = np.zeros(n, np.uint32)
         v = StateView()
         v.n = n
         for k in STATE_FIELDS:
-            setattr(v, k, _u(out[k]) if k in ("level", "interior") else _f(out[k]))
+            setattr(v, k, _u(out[k]) if k in _U32_FIELDS else _f(out[k]))
         self._check(self._lib.sph_get_state(self._h, C.byref(v)), "sph_get_state")
         return out
 

@@ -79,7 +79,14 @@ UP = C.POINTER(C.c_uint32)
 class StateView(C.Structure):
     _fields_ = [("n", C.c_uint32), ("pos", FP), ("vel", FP), ("ev", FP), ("acc", FP),
                 ("dens", FP), ("press", FP), ("energy", FP), ("surface", FP),
-                ("level", UP), ("interior", UP)]
+                ("level", UP), ("interior", UP), ("scene", UP)]
+
+
+class Scene(C.Structure):
+    _fields_ = [("lo", F3), ("hi", F3), ("viscosity", C.c_float), ("gas_constant", C.c_float)]
+
+
+SCENE_GAP_CELLS = 2
 
 
 class DebugView(C.Structure):
@@ -106,6 +113,7 @@ SIGNATURES = [
     ("sph_add_particles", C.c_int, [H, C.c_uint32, FP, FP, UP]),
     ("sph_set_state", C.c_int, [H, C.POINTER(StateView)]),
     ("sph_step", C.c_int, [H, C.c_int]),
+    ("sph_set_scenes", C.c_int, [H, C.c_uint32, C.POINTER(Scene)]),
     ("sph_set_graph", C.c_int, [H, C.c_int]),
     ("sph_sync", C.c_int, [H]),
     ("sph_get_num_particles", C.c_int, [H, UP]),

@@ -14,6 +14,7 @@
 
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -62,6 +63,10 @@ struct sph_handle {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     uint32_t graph_grid[2] = {0, 0};
     uint32_t graph_launches[2] = {0, 0};
+    // batched scenes: device table of 2 float4 per scene (own allocation,
+    // replaced by sph_set_scenes)
+    float4 *scene_tab = nullptr;
+    uint32_t scene_tab_cap = 0;
 };
 
 namespace {
@@ -286,7 +291,7 @@ int sph_create(const sph_config *cfg, sph_handle **out)
         rc |= dalloc(h, &q.ev, cap); rc |= dalloc(h, &q.acc, cap);
         rc |= dalloc(h, &q.dens, cap); rc |= dalloc(h, &q.press, cap);
         rc |= dalloc(h, &q.energy, cap); rc |= dalloc(h, &q.surface, cap);
-        rc |= dalloc(h, &q.interior, cap);
+        rc |= dalloc(h, &q.interior, cap); rc |= dalloc(h, &q.scene, cap);
     }
     WorkPtrs &w = h->w;
     rc |= dalloc(h, &h->cnt, 2);
@@ -299,7 +304,9 @@ int sph_create(const sph_config *cfg, sph_handle **out)
     rc |= dalloc(h, &w.sacc_n, cap);
     rc |= dalloc(h, &w.ssurf, cap); rc |= dalloc(h, &w.senergy, cap);
     rc |= dalloc(h, &w.snbr, cap); rc |= dalloc(h, &w.sinter, cap);
-    rc |= dalloc(h, &w.stv, cap);
+    rc |= dalloc(h, &w.stv, cap); rc |= dalloc(h, &w.sscene, cap);
+    w.scene_tab = nullptr;
+    w.nscenes = 0;
     rc |= dalloc(h, &w.split_c, cap); rc |= dalloc(h, &w.removed_c, cap);
     rc |= dalloc(h, &w.split_rank, cap); rc |= dalloc(h, &w.removed_rank, cap);
     rc |= dalloc(h, &w.split_list, cap); rc |= dalloc(h, &w.leader, cap);
@@ -334,6 +341,7 @@ int sph_destroy(sph_handle *h)
         cudaEventDestroy(h->rb_done[1]);
     }
     for (void *p : h->allocs) cudaFree(p);
+    if (h->scene_tab) cudaFree(h->scene_tab);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return SPH_OK;
@@ -394,6 +402,7 @@ int sph_add_particles(sph_handle *h, uint32_t n, const float *pos, const float *
     cudaMemcpyAsync(b.energy + n0, zf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(b.surface + n0, zf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(b.interior + n0, zu.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.scene + n0, zu.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s);
     cudaStreamSynchronize(s);
     write_n(h, n0 + n);
     h->n_ub = n0 + n;
@@ -407,6 +416,9 @@ int sph_set_state(sph_handle *h, const sph_state_view *st)
     const uint32_t n = st->n;
     if (n > h->cap) { h->err = "sph_set_state: capacity exceeded"; return SPH_ERR_CAPACITY; }
     if (n && (!st->pos || !st->level)) return SPH_ERR_INVALID;
+    if (st->scene && h->w.nscenes)
+        for (uint32_t i = 0; i < n; ++i)
+            if (st->scene[i] >= h->w.nscenes) { h->err = "sph_set_state: scene index out of range"; return SPH_ERR_RANGE; }
     const int dim = (int)h->cfg.dim;
     std::vector<float4> p4, v4, e4, a4;
     pack4(st->pos, dim, n, p4, st->level);
@@ -427,6 +439,7 @@ int sph_set_state(sph_handle *h, const sph_state_view *st)
     cudaMemcpyAsync(b.surface, st->surface ? st->surface : zf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(b.interior, st->interior ? st->interior : zu.data(), sizeof(uint32_t) * n,
                     cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b.scene, st->scene ? st->scene : zu.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s);
     cudaStreamSynchronize(s);
     write_n(h, n);
     h->n_ub = n;
@@ -519,6 +532,68 @@ int sph_set_graph(sph_handle *h, int on)
     return SPH_OK;
 }
 
+int sph_set_scenes(sph_handle *h, uint32_t nscenes, const sph_scene *scenes)
+{
+    if (!h || (nscenes && !scenes)) return SPH_ERR_INVALID;
+    const sph_config &c = h->cfg;
+    const uint32_t dim = c.dim;
+    const float gap = SPH_SCENE_GAP_CELLS * c.cell_size;
+    for (uint32_t s = 0; s < nscenes; ++s) {
+        const sph_scene &a = scenes[s];
+        if (!std::isfinite(a.viscosity) || !std::isfinite(a.gas_constant)) {
+            h->err = "sph_set_scenes: non-finite scene constant";
+            return SPH_ERR_INVALID;
+        }
+        for (uint32_t d = 0; d < dim; ++d)
+            if (!(a.lo[d] >= 0.0f && a.hi[d] <= c.world[d] && a.hi[d] - a.lo[d] > 2.0f * c.radius[0])) {
+                h->err = "sph_set_scenes: scene box outside the world or thinner than a particle";
+                return SPH_ERR_INVALID;
+            }
+    }
+    // any two boxes are separated along some axis by the gap
+    for (uint32_t s = 0; s < nscenes; ++s)
+        for (uint32_t t = s + 1; t < nscenes; ++t) {
+            bool apart = false;
+            for (uint32_t d = 0; d < dim && !apart; ++d)
+                apart = scenes[t].lo[d] >= scenes[s].hi[d] + gap || scenes[s].lo[d] >= scenes[t].hi[d] + gap;
+            if (!apart) {
+                h->err = "sph_set_scenes: scene boxes " + std::to_string(s) + " and " + std::to_string(t) +
+                         " are closer than SPH_SCENE_GAP_CELLS cells";
+                return SPH_ERR_INVALID;
+            }
+        }
+    sph_readback_wait(h);
+    const uint32_t n = read_n(h);
+    if (nscenes && n) {   // scene indices already held must name a scene
+        std::vector<uint32_t> ids(n);
+        cudaMemcpy(ids.data(), h->buf[h->cur].scene, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
+        for (uint32_t i = 0; i < n; ++i)
+            if (ids[i] >= nscenes) { h->err = "sph_set_scenes: a particle's scene index is out of range"; return SPH_ERR_RANGE; }
+    }
+    cudaStreamSynchronize(h->stream);
+    if (nscenes > h->scene_tab_cap) {
+        if (h->scene_tab) cudaFree(h->scene_tab);
+        h->scene_tab = nullptr;
+        h->scene_tab_cap = 0;
+        if (cudaMalloc(&h->scene_tab, sizeof(float4) * 2 * nscenes) != cudaSuccess)
+            return cuda_check(h, "sph_set_scenes");
+        h->scene_tab_cap = nscenes;
+    }
+    if (nscenes) {
+        std::vector<float4> tab(2 * (size_t)nscenes);
+        for (uint32_t s = 0; s < nscenes; ++s) {
+            const sph_scene &a = scenes[s];
+            tab[2 * s] = make_float4(a.lo[0], a.lo[1], dim == 3 ? a.lo[2] : 0.0f, a.viscosity);
+            tab[2 * s + 1] = make_float4(a.hi[0], a.hi[1], dim == 3 ? a.hi[2] : 0.0f, a.gas_constant);
+        }
+        cudaMemcpy(h->scene_tab, tab.data(), sizeof(float4) * tab.size(), cudaMemcpyHostToDevice);
+    }
+    h->w.scene_tab = nscenes ? h->scene_tab : nullptr;
+    h->w.nscenes = nscenes;
+    drop_graphs(h);   // captured steps hold the work pointers as arguments
+    return cuda_check(h, "sph_set_scenes");
+}
+
 int sph_sync(sph_handle *h)
 {
     if (!h) return SPH_ERR_INVALID;
@@ -576,6 +651,7 @@ int sph_get_state(sph_handle *h, sph_state_view *st)
     if (st->energy) cudaMemcpy(st->energy, b.energy, sizeof(float) * n, cudaMemcpyDeviceToHost);
     if (st->surface) cudaMemcpy(st->surface, b.surface, sizeof(float) * n, cudaMemcpyDeviceToHost);
     if (st->interior) cudaMemcpy(st->interior, b.interior, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
+    if (st->scene) cudaMemcpy(st->scene, b.scene, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
     return cuda_check(h, "sph_get_state");
 }
 
@@ -662,6 +738,10 @@ int sph_write_particles(sph_handle *h, const void *host_src, uint32_t n)
 {
     if (!h || (n && !host_src)) return SPH_ERR_INVALID;
     if (n > h->cap) { h->err = "sph_write_particles: capacity exceeded"; return SPH_ERR_CAPACITY; }
+    if (h->w.nscenes) {
+        h->err = "sph_write_particles: the record format carries no scene index (use sph_set_state)";
+        return SPH_ERR_INVALID;
+    }
     sph_readback_wait(h);
     if (int rc = ensure_aos(h)) return rc;
     const uint64_t rec = sph_particle_record_size(h);

@@ -40,6 +40,7 @@ struct CanonPtrs {
     float4 *pos, *vel, *ev, *acc;
     float *dens, *press, *energy, *surface;
     uint32_t *interior;
+    uint32_t *scene;                     // scene index (batched scenes)
 };
 
 struct WorkPtrs {
@@ -57,6 +58,9 @@ struct WorkPtrs {
     uint32_t *leader;                    // per sorted slot: 1 if merge survivor
     float4 *mpos, *mvel, *mev, *macc;    // merged values at the leader's slot
     float *menergy;
+    uint32_t *sscene;                    // scene index per sorted slot
+    const float4 *scene_tab;             // per scene: (lo.xyz, viscosity), (hi.xyz, gas constant)
+    uint32_t nscenes;                    // 0: one scene in [0, world]
 };
 
 // ------------------------------------------------------------ helpers
@@ -195,6 +199,7 @@ __global__ void __launch_bounds__(kThreads) k_reorder(const Counters *__restrict
         w.spos[d] = st.pos[i];
         w.svel[d] = st.vel[i];
         w.sev[d] = st.ev[i];
+        if (w.nscenes) w.sscene[d] = st.scene[i];
     }
 }
 
@@ -256,7 +261,8 @@ __global__ void __launch_bounds__(kThreads) k_density(sph_config c, const Counte
             }
         rho += c.mass[li] * poly6 * c.kernel6[li];   // self term
         float r = rho / c.rest_density;
-        float p = (r * r * r - 1.0f) * c.gas_constant;
+        const float gas = w.nscenes ? w.scene_tab[2 * min(w.sscene[s], w.nscenes - 1u) + 1].w : c.gas_constant;
+        float p = (r * r * r - 1.0f) * gas;
         w.saux[s] = make_float4(rho, p, p / (rho * rho), c.mass[li] / rho);
         w.snbr[s] = nb;
     }
@@ -284,6 +290,8 @@ __global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, cons
         const float ivis = c.kernel_h6_twice ? c.visco[li] / c.kernel6[li] : c.visco[li];
         const float igrad = -c.grad_poly6[li];
         const float ilap = c.lapc_poly6[li];
+        const uint32_t sid = w.nscenes ? min(w.sscene[s], w.nscenes - 1u) : 0u;
+        const float visc = w.nscenes ? w.scene_tab[2 * sid].w : c.viscosity;
         const uint32_t k = w.skey[s];
         uint3 q;
         q.x = k % c.ncell[0];
@@ -326,7 +334,7 @@ __global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, cons
                     }
                     const float mj = c.mass[lj];
                     const float tp = mi * mj * (ai.z + aj.z) * (ipk + jpk) * 0.5f / r;
-                    const float tv = (ai.w * aj.w) * c.viscosity * (ivk + jvk) * 0.5f;
+                    const float tv = (ai.w * aj.w) * visc * (ivk + jvk) * 0.5f;
                     fx += -rx * tp + (evj.x - evi.x) * tv;
                     fy += -ry * tp + (evj.y - evi.y) * tv;
                     if (DIM == 3) fz += -rz * tp + (evj.z - evi.z) * tv;
@@ -424,14 +432,21 @@ __global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, cons
                 }
             }
         }
-        // walls x, y, z (SPH-3D-2/sph_system.cu:285-319)
+        // walls x, y, z (SPH-3D-2/sph_system.cu:285-319); a batched scene
+        // has its own box
         {
-            float *xp = &x.x, *vp = &v.x;
-            for (int d = 0; d < DIM; ++d) {
-                const float hi_w = c.world[d] - rad;
-                if (xp[d] >= hi_w) { vp[d] *= c.wall_damping; xp[d] = hi_w; }
-                if (xp[d] < rad) { vp[d] *= c.wall_damping; xp[d] = rad; }
-            }
+            const float4 blo = w.nscenes ? w.scene_tab[2 * sid] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 bhi = w.nscenes ? w.scene_tab[2 * sid + 1]
+                                         : make_float4(c.world[0], c.world[1], c.world[2], 0.f);
+            const float damp = c.wall_damping;
+            auto wall = [&](float &xd, float &vd, float lo, float hi) {
+                const float hi_w = hi - rad, lo_w = lo + rad;
+                if (xd >= hi_w) { vd *= damp; xd = hi_w; }
+                if (xd < lo_w) { vd *= damp; xd = lo_w; }
+            };
+            wall(x.x, v.x, blo.x, bhi.x);
+            wall(x.y, v.y, blo.y, bhi.y);
+            if (DIM == 3) wall(x.z, v.z, blo.z, bhi.z);
         }
         if (c.integrator != SPH_INTEGRATE_REF2D) {
             ev.x = (ev.x + v.x) / 2.0f; ev.y = (ev.y + v.y) / 2.0f; ev.z = (ev.z + v.z) / 2.0f;
@@ -751,6 +766,8 @@ __global__ void __launch_bounds__(kThreads) k_write(sph_config c, const Counters
         out.pos[dst] = p; out.vel[dst] = v; out.ev[dst] = e; out.acc[dst] = a;
         out.dens[dst] = aux.x; out.press[dst] = aux.y; out.energy[dst] = en; out.surface[dst] = sf;
         out.interior[dst] = inter;
+        const uint32_t sid = w.nscenes ? w.sscene[s] : 0u;   // a merge group never spans scenes
+        if (w.nscenes) out.scene[dst] = sid;
         if (sp) {
             const uint32_t base = n - n_removed + w.split_rank[i] * extra;
             const float4 v0 = w.svel_n[s], e0 = w.sev_n[s], a0 = w.sacc_n[s];
@@ -765,6 +782,7 @@ __global__ void __launch_bounds__(kThreads) k_write(sph_config c, const Counters
                 out.pos[cd] = pc; out.vel[cd] = v0; out.ev[cd] = e0; out.acc[cd] = a0;
                 out.dens[cd] = aux.x; out.press[cd] = aux.y; out.energy[cd] = ec; out.surface[cd] = sf;
                 out.interior[cd] = 0u;
+                if (w.nscenes) out.scene[cd] = sid;
             }
         }
     }
@@ -846,6 +864,7 @@ __global__ void __launch_bounds__(kThreads) k_from_aos(uint32_t n, CanonPtrs st,
             st.dens[i] = o[8]; st.press[i] = o[9]; st.energy[i] = o[10]; st.surface[i] = o[12];
         }
         st.interior[i] = 0u;
+        st.scene[i] = 0u;    // the record format carries no scene index
     }
 }
 

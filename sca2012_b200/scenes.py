@@ -189,3 +189,79 @@ def dam_3d4(cfg, seed=0, sphere=65536):
 def block_3d(cfg, counts=(32, 32, 32), spacing=0.01, seed=0):
     pos = lattice(counts, spacing, np.zeros(3), seed)
     return pos, np.zeros_like(pos), np.ones(len(pos), np.uint32)
+
+
+def batch_scenes(cfg, count, seed=0, n_min=1024, n_max=65536, gap_cells=2):
+    """`count` independent dam-break scenes packed into one world for a
+    batched handle (sph_set_scenes).
+
+    Scene k draws, from the SplitMix64 streams of `seed`: a particle count
+    log-uniform in [n_min, n_max]; a block aspect ratio with each axis
+    factor log-uniform in [1/2, 2] (normalised to product 1); viscosity
+    log-uniform in [1e-3, 1e-1]; gas stiffness uniform in [1, 5].  The block
+    is a jittered lattice at spacing s = kernel[0] / 2 in the low corner of
+    its box; the box is twice the block along x, 1.5 times its height along
+    y and (3D) one cell deeper than the block along z, rounded up to whole
+    cells.  Boxes sit at whole-cell offsets, `gap_cells` apart, packed in
+    shelves over the x-z plane (3D) or the x-y plane (2D).
+
+    Returns (cfg, boxes, pos, vel, level, scene, counts): cfg is a copy with
+    world, ncell and max_particle (4x the particles) set; boxes is a list of
+    (lo, hi, viscosity, gas_constant) for Solver.set_scenes; particles are
+    scene by scene in scene order."""
+    dim = int(cfg.dim)
+    s = float(cfg.kernel[0]) * 0.5
+    cs = float(cfg.cell_size)
+    k = np.arange(count, dtype=np.uint64)
+    u_n = uniform(seed, k, 16)
+    n_target = np.exp(np.log(n_min) + u_n * (np.log(n_max) - np.log(n_min)))
+    asp = np.stack([2.0 ** (2.0 * uniform(seed, k, 17 + a) - 1.0) for a in range(dim)], 1)
+    asp /= np.prod(asp, axis=1, keepdims=True) ** (1.0 / dim)
+    mu = np.exp(np.log(1e-3) + uniform(seed, k, 21) * (np.log(1e-1) - np.log(1e-3)))
+    stiff = 1.0 + 4.0 * uniform(seed, k, 22)
+    blocks = np.maximum(4, np.rint(n_target[:, None] ** (1.0 / dim) * asp)).astype(np.int64)
+    # box extents in cells
+    ext = np.zeros((count, dim), np.int64)
+    ext[:, 0] = np.ceil(2.0 * blocks[:, 0] * s / cs - 1e-9)
+    ext[:, 1] = np.ceil(1.5 * blocks[:, 1] * s / cs - 1e-9)
+    if dim == 3:
+        ext[:, 2] = np.ceil(blocks[:, 2] * s / cs - 1e-9) + 1
+    # shelf packing: shelves run along x, stack along the last axis; in 3D
+    # every box spans y from 0
+    sec = dim - 1
+    g = gap_cells
+    width = int(max(np.sqrt(((ext[:, 0] + g) * (ext[:, sec] + g)).sum()) * 1.25, ext[:, 0].max() + g))
+    order = np.argsort(-ext[:, sec], kind="stable")
+    off = np.zeros((count, dim), np.int64)
+    cx = cz = depth = 0
+    for i in order:
+        if cx > 0 and cx + ext[i, 0] > width:
+            cz += depth + g
+            cx = depth = 0
+        off[i, 0] = cx
+        off[i, sec] = cz
+        cx += ext[i, 0] + g
+        depth = max(depth, int(ext[i, sec]))
+    top = off + ext
+    out = cfg.copy()
+    for a in range(dim):
+        out.ncell[a] = int(top[:, a].max())
+        out.world[a] = f32(out.ncell[a]) * f32(cs)
+    if dim == 2:
+        out.ncell[2] = 1
+        out.world[2] = 0.0
+    boxes, parts, scene = [], [], []
+    first = 0
+    for i in range(count):
+        lo = [f32(off[i, a]) * f32(cs) for a in range(dim)]
+        hi = [f32(top[i, a]) * f32(cs) for a in range(dim)]
+        boxes.append((lo, hi, float(f32(mu[i])), float(f32(stiff[i]))))
+        p = lattice(tuple(int(b) for b in blocks[i]), s, np.array(lo, np.float64), seed, first_index=first)
+        first += len(p)
+        parts.append(p)
+        scene.append(np.full(len(p), i, np.uint32))
+    pos = np.concatenate(parts)
+    counts = np.array([len(p) for p in parts], np.int64)
+    out.max_particle = int(4 * len(pos))
+    return (out, boxes, pos, np.zeros_like(pos), np.ones(len(pos), np.uint32),
+            np.concatenate(scene), counts)
