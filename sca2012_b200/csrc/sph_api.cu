@@ -537,7 +537,9 @@ int sph_set_scenes(sph_handle *h, uint32_t nscenes, const sph_scene *scenes)
     if (!h || (nscenes && !scenes)) return SPH_ERR_INVALID;
     const sph_config &c = h->cfg;
     const uint32_t dim = c.dim;
-    const float gap = SPH_SCENE_GAP_CELLS * c.cell_size;
+    // boxes at whole-cell offsets exactly SPH_SCENE_GAP_CELLS apart pass
+    // despite the FP32 rounding of lo and hi
+    const float gap = (SPH_SCENE_GAP_CELLS - 0.01f) * c.cell_size;
     for (uint32_t s = 0; s < nscenes; ++s) {
         const sph_scene &a = scenes[s];
         if (!std::isfinite(a.viscosity) || !std::isfinite(a.gas_constant)) {
