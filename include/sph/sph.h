@@ -323,6 +323,57 @@ int sph_readback_wait(sph_handle *h);
 int sph_sort_cells_noalloc(const sph_config *cfg, uint32_t n, const float *pos_dev, uint32_t *key_dev,
                            uint32_t *index_dev, uint32_t *cell_start_dev, uint32_t *cell_end_dev, void *stream);
 
+/*
+ * Differentiable rollout.  No counterpart in the reference (it has no
+ * gradients); the forward is sph_step itself.  Supported for the SI physics:
+ * SPH_INTEGRATE_PHYS, surface_coef 0, no obstacles or interactive forces.
+ *
+ * sph_rollout_forward advances nsteps from the current state and keeps the
+ * state at steps 0, k, 2k, ... (k = checkpoint_every) and the final state on
+ * the device.  sph_splat_loss splats the current state onto a node grid,
+ * G_g = sum_i m_i W_poly6(|x_g - x_i|, h_i), and returns
+ * loss = mean_g (G_g - target_g)^2 (target: host array, x fastest).
+ * sph_rollout_backward returns the gradient of the last loss with respect to
+ * the initial velocities and positions (host arrays, n0 x dim, in the order
+ * of the state the forward started from; NULL skips) and to the viscosity and
+ * gas constant (d_params[2s], d_params[2s+1] for scene s; one scene without
+ * batched scenes; nparams = the array's length).  It replays each checkpoint
+ * interval with its topology recorded -- cell lists, wall contacts, split
+ * flags, merge groups -- and runs the adjoint kernels back through it, so the
+ * gradient is that of the forward with its topology held fixed.  The handle
+ * is left holding the final state.  Any state change in between (step,
+ * set_state, ...) invalidates the rollout.
+ */
+typedef struct sph_loss_grid {
+    uint32_t n[3];           /* nodes per axis (n[2] = 1 in 2D) */
+    float origin[3];         /* position of node (0, 0, 0) */
+    float spacing;
+} sph_loss_grid;
+
+int sph_rollout_forward(sph_handle *h, uint32_t nsteps, uint32_t checkpoint_every);
+int sph_splat_loss(sph_handle *h, const sph_loss_grid *grid, const float *target, float *grid_out, double *loss);
+int sph_rollout_backward(sph_handle *h, float *d_vel0, float *d_pos0, double *d_params, uint32_t nparams);
+
+/* Topology of forward step `step` of the last rollout in particle indices of
+ * that step, for an independent (e.g. FP64 host) replay.  Counts are always
+ * set; each non-NULL array is filled (dens_nbr / force_nbr only when
+ * dens_cap / force_cap hold the pair counts). */
+typedef struct sph_topology_view {
+    uint32_t n, n_next, n_split, n_removed, split_on;   /* out */
+    uint32_t n_dens_pairs, n_force_pairs;               /* out */
+    uint32_t dens_cap, force_cap;                       /* in */
+    uint32_t *level;                 /* n: 1 or 2 */
+    uint32_t *dens_off, *dens_nbr;   /* n + 1 / pairs: CSR of j != i with r^2 < h_i^2 */
+    uint32_t *force_off, *force_nbr; /* n + 1 / pairs: force pairs; bit 30 = h_i - r > 0, bit 31 = h_j - r > 0 */
+    uint32_t *wall;                  /* n: bit 2d = clamped at the high wall of axis d, 2d+1 = low wall */
+    uint32_t *split;                 /* n: split this step */
+    uint32_t *dst;                   /* n: index of the particle's own record next step, 0xffffffff if merged away */
+    uint32_t *child;                 /* n: index of its first child record (split particles) */
+    uint32_t *merge_leader;          /* n: particle index of its merge group's leader, 0xffffffff if none */
+} sph_topology_view;
+
+int sph_rollout_topology(sph_handle *h, uint32_t step, sph_topology_view *v);
+
 /* Human-readable text of the last error on this handle (static storage). */
 const char *sph_last_error(const sph_handle *h);
 

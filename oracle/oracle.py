@@ -15,6 +15,13 @@ LIB_PATH = os.path.join(HERE, "libsph_oracle.so")
 _lib = None
 
 
+class RefTopo(C.Structure):
+    """ref_topo of sph_rollout_ref.c: one recorded step."""
+    _fields_ = [("n", C.c_uint32), ("n_next", C.c_uint32), ("split_on", C.c_uint32)] + [
+        (k, C.POINTER(C.c_uint32)) for k in ("level", "dens_off", "dens_nbr", "force_off", "force_nbr", "wall",
+                                            "split", "dst", "child", "merge_leader")]
+
+
 def _cfg_type():
     from sca2012_b200._abi import Config, StateView, DebugView
     return Config, StateView, DebugView
@@ -47,6 +54,14 @@ def load():
                                 C.POINTER(DebugView)]
     lib.oracle_step.restype = C.c_int64
     lib.oracle_density_grid.argtypes = [PC, C.c_uint32, F, U, U, U, U, D, D]
+    from sca2012_b200._abi import LossGrid
+    PT = C.POINTER(RefTopo)
+    PG = C.POINTER(LossGrid)
+    lib.ref_rollout_forward.argtypes = [PC, PT, C.c_uint32, C.c_uint32, D, D, C.c_double, C.c_double, PG, D, D]
+    lib.ref_rollout_forward.restype = C.c_double
+    lib.ref_rollout_grad.argtypes = [PC, PT, C.c_uint32, C.c_uint32, D, D, C.c_double, C.c_double, PG, D,
+                                     D, D, D, D]
+    lib.ref_rollout_grad.restype = C.c_double
     _lib = lib
     return lib
 
@@ -249,3 +264,48 @@ def density_grid(cfg, pos, level, idx, cs, ce):
     lib.oracle_density_grid(C.byref(cfg), pos.shape[0], _f(pos), _u(level), _u(idx), _u(cs), _u(ce),
                             _d(dens), _d(nrm))
     return dens, nrm
+
+
+# ----------------------------------------------------------------- FP64 rollout replay
+class Rollout64:
+    """FP64 replay of a GPU rollout with its recorded topology held fixed
+    (sph_rollout_ref.c); `topo` is the list of Solver.rollout_topology()
+    dicts of steps 0..T-1."""
+
+    def __init__(self, cfg, topo, grid_n, origin, spacing, target):
+        from sca2012_b200._abi import LossGrid
+        self.lib = load()
+        self.cfg = cfg
+        self.keep = topo
+        self.steps = (RefTopo * len(topo))()
+        for t, d in enumerate(topo):
+            st = self.steps[t]
+            st.n, st.n_next, st.split_on = d["n"], d["n_next"], d["split_on"]
+            for k in ("level", "dens_off", "dens_nbr", "force_off", "force_nbr", "wall", "split", "dst", "child",
+                      "merge_leader"):
+                setattr(st, k, _u(d[k]))
+        self.grid = LossGrid()
+        for a in range(3):
+            self.grid.n[a] = int(grid_n[a])
+            self.grid.origin[a] = float(origin[a])
+        self.grid.spacing = float(spacing)
+        self.target = np.ascontiguousarray(target, np.float64).reshape(-1)
+
+    def loss(self, x0, v0, mu, k, want_grid=False):
+        x0 = np.ascontiguousarray(x0, np.float64)
+        v0 = np.ascontiguousarray(v0, np.float64)
+        grid = np.zeros_like(self.target) if want_grid else None
+        L = self.lib.ref_rollout_forward(C.byref(self.cfg), self.steps, len(self.keep), len(x0), _d(x0), _d(v0),
+                                         float(mu), float(k), C.byref(self.grid), _d(self.target), _d(grid))
+        return (L, grid) if want_grid else L
+
+    def grad(self, x0, v0, mu, k):
+        x0 = np.ascontiguousarray(x0, np.float64)
+        v0 = np.ascontiguousarray(v0, np.float64)
+        gx = np.zeros_like(x0)
+        gv = np.zeros_like(v0)
+        gmu, gk = C.c_double(), C.c_double()
+        L = self.lib.ref_rollout_grad(C.byref(self.cfg), self.steps, len(self.keep), len(x0), _d(x0), _d(v0),
+                                      float(mu), float(k), C.byref(self.grid), _d(self.target), _d(gx), _d(gv),
+                                      C.byref(gmu), C.byref(gk))
+        return L, dict(d_pos0=gx, d_vel0=gv, d_mu=gmu.value, d_k=gk.value)

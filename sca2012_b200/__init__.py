@@ -211,6 +211,55 @@ class Solver:
         got = self.read_particles_into(buf.ctypes.data, buf.nbytes)
         return buf[: got * self.record_size].view(particle_dtype(self.dim))
 
+    # -- differentiable rollout --------------------------------------------
+    def rollout_forward(self, nsteps, checkpoint_every):
+        """Advances nsteps keeping checkpoints every `checkpoint_every` steps."""
+        self._check(self._lib.sph_rollout_forward(self._h, int(nsteps), int(checkpoint_every)),
+                    "sph_rollout_forward")
+
+    def splat_loss(self, n, origin, spacing, target):
+        """mean((G - target)^2) of the current state's density grid G (nodes
+        origin + i * spacing, x fastest); returns (loss, G)."""
+        g = _abi.LossGrid()
+        for d in range(3):
+            g.n[d] = int(n[d]) if d < self.dim else 1
+            g.origin[d] = float(origin[d]) if d < self.dim else 0.0
+        g.spacing = float(spacing)
+        tgt = np.ascontiguousarray(target, np.float32).reshape(-1)
+        grid = np.zeros_like(tgt)
+        loss = C.c_double()
+        self._check(self._lib.sph_splat_loss(self._h, C.byref(g), _f(tgt), _f(grid), C.byref(loss)),
+                    "sph_splat_loss")
+        return float(loss.value), grid
+
+    def rollout_backward(self, n0, nscenes=1):
+        """Gradient of the last splat_loss with respect to the initial
+        velocities and positions (n0 x dim) and the per-scene viscosity and
+        gas constant (nscenes x 2)."""
+        gv = np.zeros((n0, self.dim), np.float32)
+        gx = np.zeros((n0, self.dim), np.float32)
+        gp = np.zeros(2 * max(1, nscenes), np.float64)
+        self._check(self._lib.sph_rollout_backward(self._h, _f(gv), _f(gx), gp.ctypes.data_as(_abi.DP), len(gp)),
+                    "sph_rollout_backward")
+        return dict(d_vel0=gv, d_pos0=gx, d_params=gp.reshape(-1, 2))
+
+    def rollout_topology(self, step):
+        """Recorded topology of forward step `step` (particle indices of that step)."""
+        v = _abi.TopologyView()
+        self._check(self._lib.sph_rollout_topology(self._h, int(step), C.byref(v)), "sph_rollout_topology")
+        n, nd, nf = v.n, v.n_dens_pairs, v.n_force_pairs
+        out = {k: np.zeros(n, np.uint32) for k in ("level", "wall", "split", "dst", "child", "merge_leader")}
+        out["dens_off"] = np.zeros(n + 1, np.uint32)
+        out["force_off"] = np.zeros(n + 1, np.uint32)
+        out["dens_nbr"] = np.zeros(max(nd, 1), np.uint32)
+        out["force_nbr"] = np.zeros(max(nf, 1), np.uint32)
+        v.dens_cap, v.force_cap = nd, nf
+        for k, a in out.items():
+            setattr(v, k, _u(a))
+        self._check(self._lib.sph_rollout_topology(self._h, int(step), C.byref(v)), "sph_rollout_topology")
+        out.update(n=v.n, n_next=v.n_next, n_split=v.n_split, n_removed=v.n_removed, split_on=v.split_on)
+        return out
+
     # -- profiling ---------------------------------------------------------
     def set_profiling(self, on=True):
         self._check(self._lib.sph_set_profiling(self._h, 1 if on else 0), "sph_set_profiling")

@@ -100,7 +100,20 @@ class MeshView(C.Structure):
                 ("v0", FP), ("v1", FP), ("v2", FP), ("n0", FP), ("n1", FP), ("n2", FP)]
 
 
+class LossGrid(C.Structure):
+    _fields_ = [("n", U3), ("origin", F3), ("spacing", C.c_float)]
+
+
+class TopologyView(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("n_next", C.c_uint32), ("n_split", C.c_uint32), ("n_removed", C.c_uint32),
+                ("split_on", C.c_uint32), ("n_dens_pairs", C.c_uint32), ("n_force_pairs", C.c_uint32),
+                ("dens_cap", C.c_uint32), ("force_cap", C.c_uint32),
+                ("level", UP), ("dens_off", UP), ("dens_nbr", UP), ("force_off", UP), ("force_nbr", UP),
+                ("wall", UP), ("split", UP), ("dst", UP), ("child", UP), ("merge_leader", UP)]
+
+
 H = C.c_void_p
+DP = C.POINTER(C.c_double)
 
 # (name, restype, argtypes) of every entry point declared in include/sph/sph.h
 SIGNATURES = [
@@ -134,6 +147,10 @@ SIGNATURES = [
     ("sph_write_pov_particles", C.c_int, [FP, UP, C.c_uint32, C.c_uint32, FP, FP, C.c_char_p]),
     ("sph_read_particles_async", C.c_int, [H, C.c_void_p, C.c_uint64, C.c_void_p]),
     ("sph_readback_wait", C.c_int, [H]),
+    ("sph_rollout_forward", C.c_int, [H, C.c_uint32, C.c_uint32]),
+    ("sph_splat_loss", C.c_int, [H, C.POINTER(LossGrid), FP, FP, DP]),
+    ("sph_rollout_backward", C.c_int, [H, FP, FP, DP, C.c_uint32]),
+    ("sph_rollout_topology", C.c_int, [H, C.c_uint32, C.POINTER(TopologyView)]),
     ("sph_last_error", C.c_char_p, [H]),
     ("sph_sort_cells_noalloc", C.c_int, [C.POINTER(Config), C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p]),

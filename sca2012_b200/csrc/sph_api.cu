@@ -22,6 +22,8 @@
 
 using namespace sph;
 
+struct Rollout;   // differentiable rollout state (sph_rollout_impl.cuh)
+
 struct sph_handle {
     sph_config cfg;
     int device = 0;
@@ -67,11 +69,16 @@ struct sph_handle {
     // replaced by sph_set_scenes)
     float4 *scene_tab = nullptr;
     uint32_t scene_tab_cap = 0;
+    // differentiable rollout; state_gen counts state and config changes made
+    // outside of steps, so a rollout can tell it still describes the state
+    Rollout *ro = nullptr;
+    uint64_t state_gen = 0;
 };
 
 namespace {
 
 const char *kNoHandle = "null handle";
+void rollout_free(Rollout *r);
 
 template <typename T> int dalloc(sph_handle *h, T **p, size_t count)
 {
@@ -307,6 +314,9 @@ int sph_create(const sph_config *cfg, sph_handle **out)
     rc |= dalloc(h, &w.stv, cap); rc |= dalloc(h, &w.sscene, cap);
     w.scene_tab = nullptr;
     w.nscenes = 0;
+    w.merge_to = nullptr;
+    w.mvs = nullptr;
+    w.wall = nullptr;
     rc |= dalloc(h, &w.split_c, cap); rc |= dalloc(h, &w.removed_c, cap);
     rc |= dalloc(h, &w.split_rank, cap); rc |= dalloc(h, &w.removed_rank, cap);
     rc |= dalloc(h, &w.split_list, cap); rc |= dalloc(h, &w.leader, cap);
@@ -340,6 +350,7 @@ int sph_destroy(sph_handle *h)
         cudaEventDestroy(h->rb_done[0]);
         cudaEventDestroy(h->rb_done[1]);
     }
+    rollout_free(h->ro);
     for (void *p : h->allocs) cudaFree(p);
     if (h->scene_tab) cudaFree(h->scene_tab);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -362,6 +373,7 @@ int sph_set_config(sph_handle *h, const sph_config *cfg)
         return SPH_ERR_INVALID;
     }
     h->cfg = *cfg;
+    h->state_gen++;
     // captured steps hold the old constants as kernel arguments
     for (int p = 0; p < 2; ++p) {
         if (h->graph[p]) cudaGraphExecDestroy(h->graph[p]);
@@ -406,6 +418,7 @@ int sph_add_particles(sph_handle *h, uint32_t n, const float *pos, const float *
     cudaStreamSynchronize(s);
     write_n(h, n0 + n);
     h->n_ub = n0 + n;
+    h->state_gen++;
     return cuda_check(h, "sph_add_particles");
 }
 
@@ -444,6 +457,7 @@ int sph_set_state(sph_handle *h, const sph_state_view *st)
     write_n(h, n);
     h->n_ub = n;
     h->have_step = false;
+    h->state_gen++;
     return cuda_check(h, "sph_set_state");
 }
 
@@ -592,6 +606,7 @@ int sph_set_scenes(sph_handle *h, uint32_t nscenes, const sph_scene *scenes)
     }
     h->w.scene_tab = nscenes ? h->scene_tab : nullptr;
     h->w.nscenes = nscenes;
+    h->state_gen++;
     drop_graphs(h);   // captured steps hold the work pointers as arguments
     return cuda_check(h, "sph_set_scenes");
 }
@@ -758,6 +773,7 @@ int sph_write_particles(sph_handle *h, const void *host_src, uint32_t n)
     cudaStreamSynchronize(h->stream);
     h->n_ub = n;
     h->have_step = false;
+    h->state_gen++;
     return cuda_check(h, "sph_write_particles");
 }
 
@@ -917,3 +933,5 @@ int sph_surface_from_grid(sph_handle *h, const float *dens, const float *normal,
 }
 
 }  // extern "C"
+
+#include "sph_rollout_impl.cuh"

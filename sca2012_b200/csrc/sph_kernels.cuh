@@ -61,6 +61,9 @@ struct WorkPtrs {
     uint32_t *sscene;                    // scene index per sorted slot
     const float4 *scene_tab;             // per scene: (lo.xyz, viscosity), (hi.xyz, gas constant)
     uint32_t nscenes;                    // 0: one scene in [0, world]
+    uint32_t *merge_to;                  // taped steps only: slot -> its merge leader's slot
+    float *mvs;                          // taped steps only: leader slot -> summed member volume
+    uint32_t *wall;                      // taped steps only: wall contacts per slot
 };
 
 // ------------------------------------------------------------ helpers
@@ -439,14 +442,16 @@ __global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, cons
             const float4 bhi = w.nscenes ? w.scene_tab[2 * sid + 1]
                                          : make_float4(c.world[0], c.world[1], c.world[2], 0.f);
             const float damp = c.wall_damping;
-            auto wall = [&](float &xd, float &vd, float lo, float hi) {
+            uint32_t hit = 0;
+            auto wall = [&](float &xd, float &vd, float lo, float hi, int d) {
                 const float hi_w = hi - rad, lo_w = lo + rad;
-                if (xd >= hi_w) { vd *= damp; xd = hi_w; }
-                if (xd < lo_w) { vd *= damp; xd = lo_w; }
+                if (xd >= hi_w) { vd *= damp; xd = hi_w; hit |= 1u << (2 * d); }
+                if (xd < lo_w) { vd *= damp; xd = lo_w; hit |= 2u << (2 * d); }
             };
-            wall(x.x, v.x, blo.x, bhi.x);
-            wall(x.y, v.y, blo.y, bhi.y);
-            if (DIM == 3) wall(x.z, v.z, blo.z, bhi.z);
+            wall(x.x, v.x, blo.x, bhi.x, 0);
+            wall(x.y, v.y, blo.y, bhi.y, 1);
+            if (DIM == 3) wall(x.z, v.z, blo.z, bhi.z, 2);
+            if (w.wall) w.wall[s] = hit;   // recorded for the adjoint
         }
         if (c.integrator != SPH_INTEGRATE_REF2D) {
             ev.x = (ev.x + v.x) / 2.0f; ev.y = (ev.y + v.y) / 2.0f; ev.z = (ev.z + v.z) / 2.0f;
@@ -635,6 +640,10 @@ __device__ __forceinline__ void merge_group(const sph_config &c, const WorkPtrs 
     w.menergy[t1] = en / (float)ways;
     w.leader[t1] = 1u;
     for (uint32_t k = 1; k < ways; ++k) w.removed_c[w.sidx[g[k]]] = 1u;
+    if (w.merge_to) {   // recorded for the adjoint
+        for (uint32_t k = 0; k < ways; ++k) w.merge_to[g[k]] = t1;
+        w.mvs[t1] = Vs;
+    }
 }
 
 template <int DIM>

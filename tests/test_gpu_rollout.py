@@ -1,0 +1,146 @@
+"""Differentiable rollout on the GPU (sph_rollout_forward / sph_splat_loss /
+sph_rollout_backward), the differentiable-rollout workload at a reduced
+size: a jittered lattice block with initial velocities drawn N(0, 0.1^2),
+two-way split and merge on, a 32^3 density-grid loss against the grid of a
+run with viscosity 0.15 and stiffness 4.  Checked against the FP64 host
+replay of the recorded topology (its own adjoint, which test_rollout_ref.py
+checks against finite differences) and against FP64 central finite
+differences of that replay: gradients within 1e-3 relative."""
+import numpy as np
+import pytest
+
+import sca2012_b200 as sph
+from sca2012_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+GRID_N = (32, 32, 32)
+ORIGIN = (0.01, 0.01, 0.01)
+SPACING = 0.02
+FIELDS = ("pos", "vel", "ev", "acc", "dens", "press", "energy", "surface", "level", "interior")
+
+
+def _case(counts, seed, merge_steps):
+    cfg = sph.preset(sph.PRESET_ROLLOUT_3D)
+    cfg.merge_interior_steps = merge_steps
+    pos, _, lvl = scenes.block_3d(cfg, counts=counts, spacing=0.01, seed=seed)
+    pos = pos + np.float32(0.1)   # away from the low walls
+    rng = np.random.default_rng(seed)
+    vel = rng.normal(0.0, 0.1, pos.shape).astype(np.float32)
+    return cfg, pos, vel, lvl
+
+
+def _target(cfg, pos, vel, lvl, T):
+    t = cfg.copy()
+    t.viscosity, t.gas_constant = 0.15, 4.0
+    s = sph.Solver(t)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    s.step(T)
+    _, grid = s.splat_loss(GRID_N, ORIGIN, SPACING, np.zeros(np.prod(GRID_N), np.float32))
+    s.close()
+    return grid
+
+
+@pytest.fixture(scope="module")
+def rollout():
+    from oracle import oracle as O
+    T, every = 30, 7
+    cfg, pos, vel, lvl = _case((8, 8, 8), 3, 5)
+    target = _target(cfg, pos, vel, lvl, T)
+    s = sph.Solver(cfg)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    s.rollout_forward(T, every)
+    L, grid = s.splat_loss(GRID_N, ORIGIN, SPACING, target)
+    g = s.rollout_backward(len(pos))
+    final = s.get_state()
+    topo = [s.rollout_topology(t) for t in range(T)]
+    g2 = s.rollout_backward(len(pos))
+    after = s.get_state()
+    s.close()
+    rep = O.Rollout64(cfg, topo, GRID_N, ORIGIN, SPACING, target)
+    return dict(cfg=cfg, pos=pos, vel=vel, lvl=lvl, T=T, L=L, g=g, g2=g2, final=final, after=after,
+                topo=topo, rep=rep, target=target)
+
+
+def test_taping_leaves_forward_unchanged(gpu, rollout):
+    r = rollout
+    s = sph.Solver(r["cfg"])
+    s.set_state(dict(pos=r["pos"], vel=r["vel"], level=r["lvl"]))
+    s.step(r["T"])
+    plain = s.get_state()
+    s.close()
+    for f in FIELDS:
+        assert plain[f].tobytes() == r["final"][f].tobytes(), f
+        assert plain[f].tobytes() == r["after"][f].tobytes(), f
+    # the case covers adaptivity
+    assert sum(int(t["split"].sum()) for t in r["topo"]) > 0
+    assert sum(int((t["merge_leader"] != 0xFFFFFFFF).sum()) for t in r["topo"]) > 0
+
+
+def test_backward_is_repeatable(gpu, rollout):
+    r = rollout
+    assert r["g"]["d_vel0"].tobytes() == r["g2"]["d_vel0"].tobytes()
+    np.testing.assert_allclose(r["g"]["d_params"], r["g2"]["d_params"], rtol=1e-12)
+
+
+def test_gradient_matches_fp64_replay(gpu, rollout):
+    r = rollout
+    cfg = r["cfg"]
+    mu, k = float(cfg.viscosity), float(cfg.gas_constant)
+    L64, g64 = r["rep"].grad(r["pos"].astype(np.float64), r["vel"].astype(np.float64), mu, k)
+    assert abs(r["L"] - L64) <= 1e-4 * abs(L64), (r["L"], L64)
+    g = r["g"]
+    for key in ("d_vel0", "d_pos0"):
+        a, b = g[key].astype(np.float64), g64[key]
+        err = np.linalg.norm(a - b) / np.linalg.norm(b)
+        assert err <= 1e-3, (key, err)
+    assert abs(g["d_params"][0, 0] - g64["d_mu"]) <= 1e-3 * abs(g64["d_mu"]), (g["d_params"][0, 0], g64["d_mu"])
+    assert abs(g["d_params"][0, 1] - g64["d_k"]) <= 1e-3 * abs(g64["d_k"]), (g["d_params"][0, 1], g64["d_k"])
+
+
+def test_gradient_matches_finite_differences(gpu, rollout):
+    """FP64 central differences (eps 1e-6) of the replay on random
+    directions in (initial velocities, viscosity, stiffness)."""
+    r = rollout
+    cfg = r["cfg"]
+    mu, k = float(cfg.viscosity), float(cfg.gas_constant)
+    x0 = r["pos"].astype(np.float64)
+    v0 = r["vel"].astype(np.float64)
+    L = r["rep"].loss(x0, v0, mu, k)
+    rng = np.random.default_rng(11)
+    eps = 1e-6
+    noise = 50 * np.finfo(np.float64).eps * abs(L) / eps
+    g = r["g"]
+    for _ in range(8):
+        dv = rng.normal(size=v0.shape)
+        dmu, dk = rng.normal() * 0.1, rng.normal()
+        nrm = np.sqrt((dv * dv).sum() + dmu * dmu + dk * dk)
+        dv, dmu, dk = dv / nrm, dmu / nrm, dk / nrm
+        lp = r["rep"].loss(x0, v0 + eps * dv, mu + eps * dmu, k + eps * dk)
+        lm = r["rep"].loss(x0, v0 - eps * dv, mu - eps * dmu, k - eps * dk)
+        fd = (lp - lm) / (2 * eps)
+        ad = (g["d_vel0"] * dv).sum() + g["d_params"][0, 0] * dmu + g["d_params"][0, 1] * dk
+        assert abs(ad - fd) <= 1e-3 * abs(fd) + noise, (ad, fd)
+
+
+def test_rollout_errors(gpu):
+    cfg = sph.preset(sph.PRESET_REF_3D2)   # reference integrator: not covered
+    s = sph.Solver(cfg)
+    pos, vel, lvl = scenes.ref_box_3d2(cfg)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    with pytest.raises(sph.SphError):
+        s.rollout_forward(4, 2)
+    s.close()
+    cfg, pos, vel, lvl = _case((4, 4, 4), 1, 50)
+    s = sph.Solver(cfg)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    with pytest.raises(sph.SphError):   # no rollout yet
+        s.rollout_backward(len(pos))
+    s.rollout_forward(4, 2)
+    with pytest.raises(sph.SphError):   # no loss yet
+        s.rollout_backward(len(pos))
+    s.splat_loss(GRID_N, ORIGIN, SPACING, np.zeros(np.prod(GRID_N), np.float32))
+    s.step(1)
+    with pytest.raises(sph.SphError):   # the state moved on
+        s.rollout_backward(len(pos))
+    s.close()
