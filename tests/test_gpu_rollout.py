@@ -1,8 +1,9 @@
 """Differentiable rollout on the GPU (sph_rollout_forward / sph_splat_loss /
 sph_rollout_backward), the differentiable-rollout workload at a reduced
-size: a jittered lattice block with initial velocities drawn N(0, 0.1^2),
-two-way split and merge on, a 32^3 density-grid loss against the grid of a
-run with viscosity 0.15 and stiffness 4.  Checked against the FP64 host
+size (512 particles instead of 32,768; 200 steps, checkpoints every 20): a
+jittered lattice block with initial velocities drawn N(0, 0.1^2), two-way
+split and merge on, a 32^3 density-grid loss against the grid of a run with
+viscosity 0.15 and stiffness 4.  Checked against the FP64 host
 replay of the recorded topology (its own adjoint, which test_rollout_ref.py
 checks against finite differences) and against FP64 central finite
 differences of that replay: gradients within 1e-3 relative."""
@@ -44,7 +45,7 @@ def _target(cfg, pos, vel, lvl, T):
 @pytest.fixture(scope="module")
 def rollout():
     from oracle import oracle as O
-    T, every = 30, 7
+    T, every = 200, 20
     cfg, pos, vel, lvl = _case((8, 8, 8), 3, 5)
     target = _target(cfg, pos, vel, lvl, T)
     s = sph.Solver(cfg)
@@ -88,7 +89,7 @@ def test_gradient_matches_fp64_replay(gpu, rollout):
     cfg = r["cfg"]
     mu, k = float(cfg.viscosity), float(cfg.gas_constant)
     L64, g64 = r["rep"].grad(r["pos"].astype(np.float64), r["vel"].astype(np.float64), mu, k)
-    assert abs(r["L"] - L64) <= 1e-4 * abs(L64), (r["L"], L64)
+    assert abs(r["L"] - L64) <= 1e-3 * abs(L64), (r["L"], L64)
     g = r["g"]
     for key in ("d_vel0", "d_pos0"):
         a, b = g[key].astype(np.float64), g64[key]
