@@ -67,6 +67,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--batch-scenes", type=int, default=256, help="0 skips the batched-scenes comparison")
     p.add_argument("--batch-steps", type=int, default=20)
+    p.add_argument("--rollout-steps", type=int, default=200, help="0 skips the differentiable-rollout timing")
     return p.parse_args()
 
 
@@ -306,6 +307,7 @@ def run_ours(args, rank, world, local_rank):
     small["particles_initial"] = len(rpos)
 
     batched = batched_scenes(args) if (world == 1 and args.batch_scenes) else None
+    roll = rollout_bench(args) if (world == 1 and args.rollout_steps) else None
 
     out = None
     if rank == 0:
@@ -336,6 +338,7 @@ def run_ours(args, rank, world, local_rank):
             "stages_ms": stage_avg,
             "ref_3d2_default_scene": small,
             "batched_scenes": batched,
+            "rollout": roll,
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": launches,
@@ -423,6 +426,66 @@ def batched_scenes(args):
             "batched_vs_sequential": v_b / v_s, "batched_vs_concurrent_streams": v_b / v_c,
             "batched_ms_per_step": t_batched / steps * 1e3, "status": status,
             "timing": "wall clock around synchronised step loops"}
+
+
+# ----------------------------------------------------------------- differentiable rollout
+def rollout_bench(args):
+    """Differentiable-rollout workload: a 32^3 block (spacing 0.01) in the
+    0.64^3 box, initial velocities N(0, 0.1^2), two-way split/merge on, 200
+    steps with checkpoints every 20, a 32^3 density-grid loss against the
+    grid of a run with viscosity 0.15 and stiffness 4.  Reports the plain
+    forward (eager steps), the checkpointed forward, and the backward (the
+    taped replay of every interval plus the adjoint kernels), each per step;
+    wall clock around synchronised calls."""
+    import torch
+    import sca2012_b200 as sph
+    from sca2012_b200 import scenes as sc
+    T, every = args.rollout_steps, 20
+    cfg = sph.preset(sph.PRESET_ROLLOUT_3D)
+    pos, _, lvl = sc.block_3d(cfg, counts=(32, 32, 32), spacing=0.01, seed=args.seed)
+    vel = np.random.default_rng(args.seed).normal(0.0, 0.1, pos.shape).astype(np.float32)
+    gn, org, sp = (32, 32, 32), (0.01, 0.01, 0.01), 0.02
+    tcfg = cfg.copy()
+    tcfg.viscosity, tcfg.gas_constant = 0.15, 4.0
+    ts = sph.Solver(tcfg)
+    ts.set_state(dict(pos=pos, vel=vel, level=lvl))
+    ts.step(T)
+    _, target = ts.splat_loss(gn, org, sp, np.zeros(32 ** 3, np.float32))
+    ts.close()
+
+    def wall(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    s = sph.Solver(cfg)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    s.step(3)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    t_plain = wall(lambda: (s.step(T), s.sync()))
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    s.rollout_forward(T, every)     # warm-up (allocations)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    t_fwd = wall(lambda: s.rollout_forward(T, every))
+    n_final = s.num_particles()
+    loss = [None]
+    t_loss = wall(lambda: loss.__setitem__(0, s.splat_loss(gn, org, sp, target)[0]))
+    g = [None]
+    t_bwd = wall(lambda: g.__setitem__(0, s.rollout_backward(len(pos))))
+    status = s.sync_status()
+    s.close()
+    dp = g[0]["d_params"][0]
+    return {"particles_initial": len(pos), "particles_final": n_final, "steps": T, "checkpoint_every": every,
+            "plain_forward_ms_per_step": t_plain / T * 1e3,
+            "rollout_forward_ms_per_step": t_fwd / T * 1e3,
+            "backward_ms_per_step": t_bwd / T * 1e3,
+            "backward_vs_plain_forward": t_bwd / t_plain,
+            "loss": loss[0], "loss_ms": t_loss * 1e3,
+            "d_viscosity": float(dp[0]), "d_gas_constant": float(dp[1]),
+            "d_vel0_norm": float(np.linalg.norm(g[0]["d_vel0"])), "status": status,
+            "timing": "wall clock around synchronised calls"}
 
 
 # ----------------------------------------------------------------- reference arm
