@@ -141,6 +141,8 @@ typedef struct sph_config {
     uint32_t grid_every;     /* density grid + surface inside every k-th step (0: never); the
                                 reference's display mode 2 is 1 (SPH-3D-2/sph_system.cpp:336-362) */
     uint32_t max_triangles;  /* device mesh capacity (0: 3 per grid node) */
+    uint32_t compensated_positions; /* 1: positions carry an FP32 low part and x += v dt is a
+                                       compensated (Fast2Sum) update; 0: plain FP32 (reference) */
 } sph_config;
 
 /* Host view of a particle state (SoA).  Vectors hold `dim` floats per
@@ -370,6 +372,7 @@ typedef struct sph_topology_view {
     uint32_t *dst;                   /* n: index of the particle's own record next step, 0xffffffff if merged away */
     uint32_t *child;                 /* n: index of its first child record (split particles) */
     uint32_t *merge_leader;          /* n: particle index of its merge group's leader, 0xffffffff if none */
+    float *pos, *vel, *ev;           /* n x dim: the state the step started from */
 } sph_topology_view;
 
 int sph_rollout_topology(sph_handle *h, uint32_t step, sph_topology_view *v);

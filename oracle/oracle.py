@@ -19,7 +19,8 @@ class RefTopo(C.Structure):
     """ref_topo of sph_rollout_ref.c: one recorded step."""
     _fields_ = [("n", C.c_uint32), ("n_next", C.c_uint32), ("split_on", C.c_uint32)] + [
         (k, C.POINTER(C.c_uint32)) for k in ("level", "dens_off", "dens_nbr", "force_off", "force_nbr", "wall",
-                                            "split", "dst", "child", "merge_leader")]
+                                            "split", "dst", "child", "merge_leader")] + [
+        (k, C.POINTER(C.c_float)) for k in ("x_rec", "v_rec", "ev_rec")]
 
 
 def _cfg_type():
@@ -62,6 +63,9 @@ def load():
     lib.ref_rollout_grad.argtypes = [PC, PT, C.c_uint32, C.c_uint32, D, D, C.c_double, C.c_double, PG, D,
                                      D, D, D, D]
     lib.ref_rollout_grad.restype = C.c_double
+    lib.ref_rollout_grad_along.argtypes = [PC, PT, C.c_uint32, C.c_uint32, D, D, C.c_double, C.c_double, PG, D,
+                                           F, D, D, D, D]
+    lib.ref_rollout_grad_along.restype = C.c_double
     _lib = lib
     return lib
 
@@ -284,6 +288,9 @@ class Rollout64:
             for k in ("level", "dens_off", "dens_nbr", "force_off", "force_nbr", "wall", "split", "dst", "child",
                       "merge_leader"):
                 setattr(st, k, _u(d[k]))
+            for k, src in (("x_rec", "pos"), ("v_rec", "vel"), ("ev_rec", "ev")):
+                if src in d:
+                    setattr(st, k, _f(d[src]))
         self.grid = LossGrid()
         for a in range(3):
             self.grid.n[a] = int(grid_n[a])
@@ -308,4 +315,18 @@ class Rollout64:
         L = self.lib.ref_rollout_grad(C.byref(self.cfg), self.steps, len(self.keep), len(x0), _d(x0), _d(v0),
                                       float(mu), float(k), C.byref(self.grid), _d(self.target), _d(gx), _d(gv),
                                       C.byref(gmu), C.byref(gk))
+        return L, dict(d_pos0=gx, d_vel0=gv, d_mu=gmu.value, d_k=gk.value)
+
+    def grad_along(self, x0, v0, mu, k, x_final):
+        """FP64 adjoint linearised about the recorded FP32 trajectory (the
+        topology dicts must carry pos/vel/ev; x_final = the final positions)."""
+        x0 = np.ascontiguousarray(x0, np.float64)
+        v0 = np.ascontiguousarray(v0, np.float64)
+        xf = np.ascontiguousarray(x_final, np.float32)
+        gx = np.zeros_like(x0)
+        gv = np.zeros_like(v0)
+        gmu, gk = C.c_double(), C.c_double()
+        L = self.lib.ref_rollout_grad_along(C.byref(self.cfg), self.steps, len(self.keep), len(x0), _d(x0), _d(v0),
+                                            float(mu), float(k), C.byref(self.grid), _d(self.target), _f(xf),
+                                            _d(gx), _d(gv), C.byref(gmu), C.byref(gk))
         return L, dict(d_pos0=gx, d_vel0=gv, d_mu=gmu.value, d_k=gk.value)

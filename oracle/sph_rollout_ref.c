@@ -40,6 +40,7 @@
 typedef struct ref_topo {
     uint32_t n, n_next, split_on;
     const uint32_t *level, *dens_off, *dens_nbr, *force_off, *force_nbr, *wall, *split, *dst, *child, *merge_leader;
+    const float *x_rec, *v_rec, *ev_rec;   /* optional: the recorded FP32 state the step started from */
 } ref_topo;
 
 typedef struct {
@@ -275,9 +276,24 @@ double ref_rollout_forward(const sph_config *c, const ref_topo *steps, uint32_t 
     return L;
 }
 
-double ref_rollout_grad(const sph_config *c, const ref_topo *steps, uint32_t T, uint32_t n0, const double *x0,
+/* Overwrites a state with recorded FP32 values (dim per particle). */
+static void load_rec(const sph_config *c, step_rec *s, const float *x, const float *v, const float *ev)
+{
+    const int dim = (int)c->dim;
+    for (uint32_t i = 0; i < s->n; ++i)
+        for (int d = 0; d < dim; ++d) {
+            if (x) s->x[3 * i + d] = x[(size_t)i * dim + d];
+            if (v) s->v[3 * i + d] = v[(size_t)i * dim + d];
+            if (ev) s->ev[3 * i + d] = ev[(size_t)i * dim + d];
+        }
+}
+
+/* follow != 0: every step starts from its recorded FP32 state (x_rec, ...)
+ * and the loss is taken at x_final, so the FP64 adjoint is linearised about
+ * the GPU's own trajectory. */
+static double grad_impl(const sph_config *c, const ref_topo *steps, uint32_t T, uint32_t n0, const double *x0,
                         const double *v0, double mu, double kgas, const sph_loss_grid *g, const double *target,
-                        double *g_x0, double *g_v0, double *g_mu, double *g_k)
+                        double *g_x0, double *g_v0, double *g_mu, double *g_k, int follow, const float *x_final)
 {
     if (T == 0) return 0.0;
     const int dim = (int)c->dim;
@@ -285,9 +301,11 @@ double ref_rollout_grad(const sph_config *c, const ref_topo *steps, uint32_t T, 
     rec_alloc(&rec[0], n0, 1);
     init_state(c, &rec[0], n0, x0, v0);
     for (uint32_t t = 0; t < T; ++t) {
+        if (follow) load_rec(c, &rec[t], steps[t].x_rec, steps[t].v_rec, steps[t].ev_rec);
         rec_alloc(&rec[t + 1], steps[t].n_next, t + 1 < T);
         step_forward(c, &steps[t], &rec[t], &rec[t + 1], mu, kgas);
     }
+    if (follow && x_final) load_rec(c, &rec[T], x_final, NULL, NULL);
     const size_t N = (size_t)g->n[0] * g->n[1] * (dim == 3 ? g->n[2] : 1u);
     double *grid = dalloc(N), *resid = dalloc(N);
     uint32_t *lf = (uint32_t *)calloc(rec[T].n ? rec[T].n : 1, sizeof(uint32_t));
@@ -479,4 +497,18 @@ double ref_rollout_grad(const sph_config *c, const ref_topo *steps, uint32_t T, 
     for (uint32_t t = 0; t <= T; ++t) rec_free(&rec[t]);
     free(rec);
     return L;
+}
+
+double ref_rollout_grad(const sph_config *c, const ref_topo *steps, uint32_t T, uint32_t n0, const double *x0,
+                        const double *v0, double mu, double kgas, const sph_loss_grid *g, const double *target,
+                        double *g_x0, double *g_v0, double *g_mu, double *g_k)
+{
+    return grad_impl(c, steps, T, n0, x0, v0, mu, kgas, g, target, g_x0, g_v0, g_mu, g_k, 0, NULL);
+}
+
+double ref_rollout_grad_along(const sph_config *c, const ref_topo *steps, uint32_t T, uint32_t n0, const double *x0,
+                              const double *v0, double mu, double kgas, const sph_loss_grid *g, const double *target,
+                              const float *x_final, double *g_x0, double *g_v0, double *g_mu, double *g_k)
+{
+    return grad_impl(c, steps, T, n0, x0, v0, mu, kgas, g, target, g_x0, g_v0, g_mu, g_k, 1, x_final);
 }

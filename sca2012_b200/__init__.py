@@ -243,8 +243,9 @@ class Solver:
                     "sph_rollout_backward")
         return dict(d_vel0=gv, d_pos0=gx, d_params=gp.reshape(-1, 2))
 
-    def rollout_topology(self, step):
-        """Recorded topology of forward step `step` (particle indices of that step)."""
+    def rollout_topology(self, step, states=False):
+        """Recorded topology of forward step `step` (particle indices of that
+        step); states=True adds the FP32 state the step started from."""
         v = _abi.TopologyView()
         self._check(self._lib.sph_rollout_topology(self._h, int(step), C.byref(v)), "sph_rollout_topology")
         n, nd, nf = v.n, v.n_dens_pairs, v.n_force_pairs
@@ -256,6 +257,10 @@ class Solver:
         v.dens_cap, v.force_cap = nd, nf
         for k, a in out.items():
             setattr(v, k, _u(a))
+        if states:
+            for k in ("pos", "vel", "ev"):
+                out[k] = np.zeros((n, self.dim), np.float32)
+                setattr(v, k, _f(out[k]))
         self._check(self._lib.sph_rollout_topology(self._h, int(step), C.byref(v)), "sph_rollout_topology")
         out.update(n=v.n, n_next=v.n_next, n_split=v.n_split, n_removed=v.n_removed, split_on=v.split_on)
         return out

@@ -63,7 +63,7 @@ class Config(C.Structure):
         ("extern_len", C.c_float), ("extern_coe", C.c_float),
         ("dens_mul", C.c_uint32), ("den_size", C.c_float), ("ndens", U3), ("iso_value", C.c_float),
         ("mc_interpolate", C.c_uint32), ("splat_with_kernel", C.c_uint32), ("grid_every", C.c_uint32),
-        ("max_triangles", C.c_uint32),
+        ("max_triangles", C.c_uint32), ("compensated_positions", C.c_uint32),
     ]
 
     def copy(self):
@@ -109,7 +109,8 @@ class TopologyView(C.Structure):
                 ("split_on", C.c_uint32), ("n_dens_pairs", C.c_uint32), ("n_force_pairs", C.c_uint32),
                 ("dens_cap", C.c_uint32), ("force_cap", C.c_uint32),
                 ("level", UP), ("dens_off", UP), ("dens_nbr", UP), ("force_off", UP), ("force_nbr", UP),
-                ("wall", UP), ("split", UP), ("dst", UP), ("child", UP), ("merge_leader", UP)]
+                ("wall", UP), ("split", UP), ("dst", UP), ("child", UP), ("merge_leader", UP),
+                ("pos", FP), ("vel", FP), ("ev", FP)]
 
 
 H = C.c_void_p

@@ -168,6 +168,7 @@ template <int DIM> int run_step(sph_handle *h)
     const int p = h->cur;
     Counters *cin = h->cnt + p, *cout = h->cnt + (p ^ 1);
     CanonPtrs in = h->buf[p], out = h->buf[p ^ 1];
+    h->w.pos_comp = c.compensated_positions ? 1u : 0u;
     WorkPtrs w = h->w;
     const uint32_t G = grid_for(h, h->n_ub);
     cudaStream_t s = h->stream;
@@ -298,7 +299,7 @@ int sph_create(const sph_config *cfg, sph_handle **out)
         rc |= dalloc(h, &q.ev, cap); rc |= dalloc(h, &q.acc, cap);
         rc |= dalloc(h, &q.dens, cap); rc |= dalloc(h, &q.press, cap);
         rc |= dalloc(h, &q.energy, cap); rc |= dalloc(h, &q.surface, cap);
-        rc |= dalloc(h, &q.interior, cap); rc |= dalloc(h, &q.scene, cap);
+        rc |= dalloc(h, &q.interior, cap); rc |= dalloc(h, &q.scene, cap); rc |= dalloc(h, &q.pos_lo, cap);
     }
     WorkPtrs &w = h->w;
     rc |= dalloc(h, &h->cnt, 2);
@@ -312,6 +313,8 @@ int sph_create(const sph_config *cfg, sph_handle **out)
     rc |= dalloc(h, &w.ssurf, cap); rc |= dalloc(h, &w.senergy, cap);
     rc |= dalloc(h, &w.snbr, cap); rc |= dalloc(h, &w.sinter, cap);
     rc |= dalloc(h, &w.stv, cap); rc |= dalloc(h, &w.sscene, cap);
+    rc |= dalloc(h, &w.spos_lo, cap); rc |= dalloc(h, &w.spos_lo_n, cap);
+    w.pos_comp = cfg->compensated_positions ? 1u : 0u;
     w.scene_tab = nullptr;
     w.nscenes = 0;
     w.merge_to = nullptr;
@@ -372,6 +375,12 @@ int sph_set_config(sph_handle *h, const sph_config *cfg)
         h->err = "sph_set_config: density grid is fixed at creation";
         return SPH_ERR_INVALID;
     }
+    if (cfg->compensated_positions && !h->cfg.compensated_positions) {
+        // the low parts start from zero when compensation is switched on
+        sph_readback_wait(h);
+        for (int b = 0; b < 2; ++b) cudaMemsetAsync(h->buf[b].pos_lo, 0, sizeof(float4) * h->cap, h->stream);
+        cudaStreamSynchronize(h->stream);
+    }
     h->cfg = *cfg;
     h->state_gen++;
     // captured steps hold the old constants as kernel arguments
@@ -415,6 +424,7 @@ int sph_add_particles(sph_handle *h, uint32_t n, const float *pos, const float *
     cudaMemcpyAsync(b.surface + n0, zf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(b.interior + n0, zu.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(b.scene + n0, zu.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(b.pos_lo + n0, 0, sizeof(float4) * n, s);
     cudaStreamSynchronize(s);
     write_n(h, n0 + n);
     h->n_ub = n0 + n;
@@ -453,6 +463,7 @@ int sph_set_state(sph_handle *h, const sph_state_view *st)
     cudaMemcpyAsync(b.interior, st->interior ? st->interior : zu.data(), sizeof(uint32_t) * n,
                     cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(b.scene, st->scene ? st->scene : zu.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(b.pos_lo, 0, sizeof(float4) * (n ? n : 1), s);
     cudaStreamSynchronize(s);
     write_n(h, n);
     h->n_ub = n;

@@ -288,12 +288,14 @@ extern "C" int sph_config_preset(int preset, sph_config *c)
         c->grid_every = 10;  // marching cubes every 10 steps
         return SPH_OK;
     case SPH_PRESET_ROLLOUT_3D:
-        // 32^3 block at s = 0.01 in 0.64^3, two-way
+        // 32^3 block at s = 0.01 in 0.64^3, two-way; compensated positions
+        // keep the FP32 trajectory within the rounding of a few steps
         preset_si(c, 3, 0.01f, 2, 5e-5f);
         set_grid(c, 0.64f, 0.64f, 0.64f, c->kernel[0]);
         c->max_particle = 32768 * 4;
         c->use_split = 1;
         c->use_merge = 1;
+        c->compensated_positions = 1;
         set_mc_grid(c, 1);
         return SPH_OK;
     default:

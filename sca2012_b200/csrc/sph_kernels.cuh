@@ -41,6 +41,7 @@ struct CanonPtrs {
     float *dens, *press, *energy, *surface;
     uint32_t *interior;
     uint32_t *scene;                     // scene index (batched scenes)
+    float4 *pos_lo;                      // low part of the position (compensated positions)
 };
 
 struct WorkPtrs {
@@ -64,7 +65,19 @@ struct WorkPtrs {
     uint32_t *merge_to;                  // taped steps only: slot -> its merge leader's slot
     float *mvs;                          // taped steps only: leader slot -> summed member volume
     uint32_t *wall;                      // taped steps only: wall contacts per slot
+    float4 *spos_lo, *spos_lo_n;         // low position parts per slot (compensated positions)
+    uint32_t pos_comp;                   // the config's compensated_positions
 };
+
+// hi + lo += d with hi, lo FP32 (Fast2Sum; |hi| >= |d + lo| holds for a
+// position and one step's displacement).
+__device__ __forceinline__ void comp_add(float &hi, float &lo, float d)
+{
+    const float y = __fadd_rn(d, lo);
+    const float t = __fadd_rn(hi, y);
+    lo = __fadd_rn(__fsub_rn(hi, t), y);
+    hi = t;
+}
 
 // ------------------------------------------------------------ helpers
 __device__ __forceinline__ int lv(float w) { return w == 1.0f ? 0 : 1; }
@@ -203,6 +216,7 @@ __global__ void __launch_bounds__(kThreads) k_reorder(const Counters *__restrict
         w.svel[d] = st.vel[i];
         w.sev[d] = st.ev[i];
         if (w.nscenes) w.sscene[d] = st.scene[i];
+        if (w.pos_comp) w.spos_lo[d] = st.pos_lo[i];
     }
 }
 
@@ -389,6 +403,7 @@ __global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, cons
         // ---- integrate ----
         const float rho = ai.x, dt = c.time_step;
         float4 x = pi;
+        float4 lo = make_float4(0.f, 0.f, 0.f, 0.f);   // low position part (compensated positions)
         float4 v = w.svel[s];
         float4 ev = evi;
         float4 a = make_float4(fx, fy, fz, 0.f);
@@ -417,7 +432,14 @@ __global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, cons
                 v.y += (a.y * im + c.gravity[1]) * dt;
                 v.z += (a.z * im + c.gravity[2]) * dt;
             }
-            x.x += v.x * dt; x.y += v.y * dt; x.z += v.z * dt;
+            if (w.pos_comp) {
+                lo = w.spos_lo[s];
+                comp_add(x.x, lo.x, __fmul_rn(v.x, dt));
+                comp_add(x.y, lo.y, __fmul_rn(v.y, dt));
+                if (DIM == 3) comp_add(x.z, lo.z, __fmul_rn(v.z, dt));
+            } else {
+                x.x += v.x * dt; x.y += v.y * dt; x.z += v.z * dt;
+            }
             if (DIM == 3 && c.use_cylinder) {   // SPH-3D-2/sph_system.cu:242-282
                 for (int qq = 0; qq < 3; ++qq) {
                     const sph_sphere S = c.sphere[qq];
@@ -429,6 +451,7 @@ __global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, cons
                         float il = rsqrtf(sx * sx + sy * sy + sz * sz);
                         float nx = sx * il, ny = sy * il, nz = sz * il;
                         x.x = S.pos[0] + sx; x.y = S.pos[1] + sy; x.z = S.pos[2] + sz;
+                        lo = make_float4(0.f, 0.f, 0.f, 0.f);
                         float vn = v.x * nx + v.y * ny + v.z * nz;
                         v.x -= S.damping * vn * nx; v.y -= S.damping * vn * ny; v.z -= S.damping * vn * nz;
                     }
@@ -443,20 +466,21 @@ __global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, cons
                                          : make_float4(c.world[0], c.world[1], c.world[2], 0.f);
             const float damp = c.wall_damping;
             uint32_t hit = 0;
-            auto wall = [&](float &xd, float &vd, float lo, float hi, int d) {
-                const float hi_w = hi - rad, lo_w = lo + rad;
-                if (xd >= hi_w) { vd *= damp; xd = hi_w; hit |= 1u << (2 * d); }
-                if (xd < lo_w) { vd *= damp; xd = lo_w; hit |= 2u << (2 * d); }
+            auto wall = [&](float &xd, float &vd, float &xl, float lo_b, float hi_b, int d) {
+                const float hi_w = hi_b - rad, lo_w = lo_b + rad;
+                if (xd >= hi_w) { vd *= damp; xd = hi_w; xl = 0.0f; hit |= 1u << (2 * d); }
+                if (xd < lo_w) { vd *= damp; xd = lo_w; xl = 0.0f; hit |= 2u << (2 * d); }
             };
-            wall(x.x, v.x, blo.x, bhi.x, 0);
-            wall(x.y, v.y, blo.y, bhi.y, 1);
-            if (DIM == 3) wall(x.z, v.z, blo.z, bhi.z, 2);
+            wall(x.x, v.x, lo.x, blo.x, bhi.x, 0);
+            wall(x.y, v.y, lo.y, blo.y, bhi.y, 1);
+            if (DIM == 3) wall(x.z, v.z, lo.z, blo.z, bhi.z, 2);
             if (w.wall) w.wall[s] = hit;   // recorded for the adjoint
         }
         if (c.integrator != SPH_INTEGRATE_REF2D) {
             ev.x = (ev.x + v.x) / 2.0f; ev.y = (ev.y + v.y) / 2.0f; ev.z = (ev.z + v.z) / 2.0f;
         }
         w.spos_n[s] = x;        // .w keeps the level
+        if (w.pos_comp) w.spos_lo_n[s] = lo;
         w.svel_n[s] = v;
         w.sev_n[s] = ev;
         w.sacc_n[s] = a;
@@ -766,7 +790,10 @@ __global__ void __launch_bounds__(kThreads) k_write(sph_config c, const Counters
             if (ways == 4) en = en / 4.0f;
             inter = 0u;
         }
+        float4 plo = w.pos_comp ? w.spos_lo_n[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 plo_pre = plo;
         if (w.leader[s]) {
+            plo = make_float4(0.f, 0.f, 0.f, 0.f);   // a merged position is a fresh FP32 mean
             p = w.mpos[s]; v = w.mvel[s]; e = w.mev[s]; a = w.macc[s];
             if (DIM == 2) en = w.menergy[s];
             inter = 0u;
@@ -777,6 +804,7 @@ __global__ void __launch_bounds__(kThreads) k_write(sph_config c, const Counters
         out.interior[dst] = inter;
         const uint32_t sid = w.nscenes ? w.sscene[s] : 0u;   // a merge group never spans scenes
         if (w.nscenes) out.scene[dst] = sid;
+        if (w.pos_comp) out.pos_lo[dst] = plo;
         if (sp) {
             const uint32_t base = n - n_removed + w.split_rank[i] * extra;
             const float4 v0 = w.svel_n[s], e0 = w.sev_n[s], a0 = w.sacc_n[s];
@@ -792,6 +820,7 @@ __global__ void __launch_bounds__(kThreads) k_write(sph_config c, const Counters
                 out.dens[cd] = aux.x; out.press[cd] = aux.y; out.energy[cd] = ec; out.surface[cd] = sf;
                 out.interior[cd] = 0u;
                 if (w.nscenes) out.scene[cd] = sid;
+                if (w.pos_comp) out.pos_lo[cd] = plo_pre;
             }
         }
     }
@@ -874,6 +903,7 @@ __global__ void __launch_bounds__(kThreads) k_from_aos(uint32_t n, CanonPtrs st,
         }
         st.interior[i] = 0u;
         st.scene[i] = 0u;    // the record format carries no scene index
+        st.pos_lo[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
 }
 

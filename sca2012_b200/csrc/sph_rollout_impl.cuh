@@ -64,6 +64,7 @@ int alloc_canon(sph_handle *h, Rollout *r, CanonPtrs &q)
     rc |= ralloc(h, r, &q.vel, n); rc |= ralloc(h, r, &q.ev, n); rc |= ralloc(h, r, &q.acc, n);
     rc |= ralloc(h, r, &q.dens, n); rc |= ralloc(h, r, &q.press, n); rc |= ralloc(h, r, &q.energy, n);
     rc |= ralloc(h, r, &q.surface, n); rc |= ralloc(h, r, &q.interior, n); rc |= ralloc(h, r, &q.scene, n);
+    rc |= ralloc(h, r, &q.pos_lo, n);
     return rc ? SPH_ERR_CUDA : SPH_OK;
 }
 
@@ -94,6 +95,7 @@ void copy_canon(const CanonPtrs &dst, const CanonPtrs &src, uint32_t n, cudaStre
     d2d(dst.acc, src.acc, n, s); d2d(dst.dens, src.dens, n, s); d2d(dst.press, src.press, n, s);
     d2d(dst.energy, src.energy, n, s); d2d(dst.surface, src.surface, n, s);
     d2d(dst.interior, src.interior, n, s); d2d(dst.scene, src.scene, n, s);
+    d2d(dst.pos_lo, src.pos_lo, n, s);
 }
 
 // Makes checkpoint k the handle's current state (all counters reset).
@@ -193,6 +195,7 @@ template <int DIM> void sort_only(sph_handle *h)
     const sph_config &c = h->cfg;
     Counters *cin = h->cnt + h->cur;
     const CanonPtrs in = h->buf[h->cur];
+    h->w.pos_comp = c.compensated_positions ? 1u : 0u;
     const WorkPtrs w = h->w;
     const uint32_t G = grid_for(h, h->n_ub);
     cudaStream_t s = h->stream;
@@ -316,7 +319,7 @@ template <int DIM> int topology_impl(sph_handle *h, Rollout *r, uint32_t step, s
     if (v->dens_off) cudaMemcpyAsync(v->dens_off, r->toff[0], sizeof(uint32_t) * (n + 1), cudaMemcpyDeviceToHost, s);
     if (v->force_off) cudaMemcpyAsync(v->force_off, r->toff[1], sizeof(uint32_t) * (n + 1), cudaMemcpyDeviceToHost, s);
     std::vector<uint32_t> inv(n), sidx(n), wall(n), split_c(n), removed_c(n), removed_rank(n), split_rank(n), mt(n);
-    std::vector<float4> spos(n);
+    std::vector<float4> spos(n), svel, sev;
     auto get = [&](void *dst, const void *src, size_t bytes) {
         if (bytes) cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
     };
@@ -324,7 +327,22 @@ template <int DIM> int topology_impl(sph_handle *h, Rollout *r, uint32_t step, s
     get(split_c.data(), t.split_c, 4ull * n); get(removed_c.data(), t.removed_c, 4ull * n);
     get(removed_rank.data(), t.removed_rank, 4ull * n); get(split_rank.data(), t.split_rank, 4ull * n);
     get(mt.data(), t.merge_to, 4ull * n); get(spos.data(), t.spos, 16ull * n);
+    if (v->vel) { svel.resize(n); get(svel.data(), t.svel, 16ull * n); }
+    if (v->ev) { sev.resize(n); get(sev.data(), t.sev, 16ull * n); }
     cudaStreamSynchronize(s);
+    const int dim = (int)c.dim;
+    auto put = [&](float *dst, const std::vector<float4> &src) {
+        if (!dst) return;
+        for (uint32_t i = 0; i < n; ++i) {
+            const float4 q = src[inv[i]];
+            dst[(size_t)i * dim] = q.x;
+            dst[(size_t)i * dim + 1] = q.y;
+            if (dim == 3) dst[(size_t)i * dim + 2] = q.z;
+        }
+    };
+    put(v->pos, spos);
+    put(v->vel, svel);
+    put(v->ev, sev);
     for (uint32_t i = 0; i < n; ++i) {
         const uint32_t sl = inv[i];
         if (v->level) v->level[i] = (uint32_t)spos[sl].w;

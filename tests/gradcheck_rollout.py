@@ -60,7 +60,8 @@ def main():
     L_gpu, _ = s.splat_loss(gn, org, sp, target)
     g = s.rollout_backward(len(pos))
     t_gpu = time.perf_counter() - t0
-    topo = [s.rollout_topology(t) for t in range(a.steps)]
+    topo = [s.rollout_topology(t, states=True) for t in range(a.steps)]
+    x_final = s.get_state()["pos"]
     n_final = s.num_particles()
     s.close()
     splits = int(sum(int(t["split"].sum()) for t in topo))
@@ -73,6 +74,9 @@ def main():
     t0 = time.perf_counter()
     L64, g64 = rep.grad(x0, v0, mu, k)
     t_ref = time.perf_counter() - t0
+    # the same FP64 adjoint about the GPU's FP32 trajectory: isolates the
+    # adjoint arithmetic from the forward's FP32 rounding
+    La, ga = rep.grad_along(x0, v0, mu, k, x_final)
 
     def rel(a_, b_):
         return float(np.linalg.norm(np.asarray(a_, np.float64) - b_) / np.linalg.norm(b_))
@@ -111,6 +115,11 @@ def main():
         "loss_gpu": L_gpu, "loss_fp64": L64, "loss_rel": abs(L_gpu - L64) / abs(L64),
         "d_vel0_rel_vs_fp64_adjoint": rel(g["d_vel0"], g64["d_vel0"]),
         "d_pos0_rel_vs_fp64_adjoint": rel(g["d_pos0"], g64["d_pos0"]),
+        "along_fp32_trajectory": {
+            "loss_rel": abs(L_gpu - La) / abs(La),
+            "d_vel0_rel": rel(g["d_vel0"], ga["d_vel0"]), "d_pos0_rel": rel(g["d_pos0"], ga["d_pos0"]),
+            "d_viscosity_rel": abs(g["d_params"][0, 0] - ga["d_mu"]) / abs(ga["d_mu"]),
+            "d_gas_constant_rel": abs(g["d_params"][0, 1] - ga["d_k"]) / abs(ga["d_k"])},
         "params": par,
         "directions": a.dirs, "eps": eps, "fd_noise_floor": noise,
         "dir_rel_gpu_vs_fd_max": float(rel_gpu.max()), "dir_rel_gpu_vs_fd_median": float(np.median(rel_gpu)),
