@@ -145,3 +145,100 @@ def test_rollout_errors(gpu):
     with pytest.raises(sph.SphError):   # the state moved on
         s.rollout_backward(len(pos))
     s.close()
+
+
+def _rollout_2d(T=120, every=25):
+    cfg = sph.preset(sph.PRESET_DAM_2D)
+    cfg.use_split = cfg.use_merge = 1
+    cfg.merge_interior_steps = 5
+    cfg.compensated_positions = 1
+    pos = scenes.lattice((16, 16), 0.01, np.array([0.1, 0.1]), 5)
+    lvl = np.ones(len(pos), np.uint32)
+    vel = np.random.default_rng(5).normal(0.0, 0.1, pos.shape).astype(np.float32)
+    gn, org, sp = (64, 64, 1), (0.005, 0.005, 0.0), 0.01
+    t = cfg.copy()
+    t.viscosity, t.gas_constant = 0.15, 4.0
+    s = sph.Solver(t)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    s.step(T)
+    _, target = s.splat_loss(gn, org, sp, np.zeros(64 * 64, np.float32))
+    s.close()
+    s = sph.Solver(cfg)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    s.rollout_forward(T, every)
+    L, _ = s.splat_loss(gn, org, sp, target)
+    g = s.rollout_backward(len(pos))
+    topo = [s.rollout_topology(k, states=True) for k in range(T)]
+    x_final = s.get_state()["pos"]
+    s.close()
+    return cfg, pos, vel, L, g, topo, (gn, org, sp, target), x_final
+
+
+def test_rollout_2d_matches_fp64(gpu):
+    """2D (plain volume means in merges, no z) against the FP64 replay."""
+    from oracle import oracle as O
+    cfg, pos, vel, L, g, topo, (gn, org, sp, target), x_final = _rollout_2d()
+    assert sum(int(t["split"].sum()) for t in topo) > 0
+    rep = O.Rollout64(cfg, topo, gn, org, sp, target)
+    mu, k = float(cfg.viscosity), float(cfg.gas_constant)
+    # the adjoint arithmetic alone: FP64 adjoint about the GPU's trajectory
+    La, ga = rep.grad_along(pos.astype(np.float64), vel.astype(np.float64), mu, k, x_final)
+    L64, g64 = rep.grad(pos.astype(np.float64), vel.astype(np.float64), mu, k)
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    info = dict(L=L, La=La, L64=L64, along=rel(g["d_vel0"], ga["d_vel0"]), fp64=rel(g["d_vel0"], g64["d_vel0"]),
+                mu=(g["d_params"][0, 0], g64["d_mu"]), k=(g["d_params"][0, 1], g64["d_k"]))
+    assert info["along"] <= 5e-4, info
+    assert abs(L - L64) <= 1e-3 * abs(L64), info
+    assert info["fp64"] <= 1e-3, info
+    assert abs(g["d_params"][0, 0] - g64["d_mu"]) <= 1e-3 * abs(g64["d_mu"]), info
+    assert abs(g["d_params"][0, 1] - g64["d_k"]) <= 1e-3 * abs(g64["d_k"]), info
+
+
+def test_batched_rollout_equals_alone(gpu):
+    """Batched scenes through the adjoint: each scene's velocity gradient is
+    bit-identical to the scene's own rollout in the same world (targets with
+    disjoint support, so the batched loss is the sum of the scenes' losses),
+    and the per-scene viscosity / stiffness gradients agree to FP64
+    rounding (their sums use FP64 atomics)."""
+    base = sph.preset(sph.PRESET_DAM_3D2)
+    base.use_split = base.use_merge = 1
+    base.merge_interior_steps = 5
+    cfg, boxes, pos, vel0, lvl, scene, counts = scenes.batch_scenes(base, 4, seed=9, n_min=512, n_max=2048)
+    vel = np.random.default_rng(9).normal(0.0, 0.1, pos.shape).astype(np.float32)
+    T, every = 40, 10
+    gn = tuple(int(cfg.ncell[a]) for a in range(3))
+    org = tuple(0.5 * float(cfg.cell_size) for _ in range(3))
+    sp = float(cfg.cell_size)
+    N = int(np.prod(gn))
+    # target: each scene run with its constants perturbed
+    tb = [(lo, hi, mu * 1.5, k + 1.0) for lo, hi, mu, k in boxes]
+    s = sph.Solver(cfg)
+    s.set_scenes(tb)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl, scene=scene))
+    s.step(T)
+    _, target = s.splat_loss(gn, org, sp, np.zeros(N, np.float32))
+    s.close()
+    s = sph.Solver(cfg)
+    s.set_scenes(boxes)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl, scene=scene))
+    s.rollout_forward(T, every)
+    Lb, _ = s.splat_loss(gn, org, sp, target)
+    gb = s.rollout_backward(len(pos), nscenes=len(boxes))
+    s.close()
+    first = np.concatenate([[0], np.cumsum(counts)])
+    La = 0.0
+    for k in range(len(boxes)):
+        c1 = cfg.copy()
+        c1.max_particle = int(4 * counts[k])
+        sl = slice(first[k], first[k + 1])
+        s = sph.Solver(c1)
+        s.set_scenes([boxes[k]])
+        s.set_state(dict(pos=pos[sl], vel=vel[sl], level=lvl[sl]))
+        s.rollout_forward(T, every)
+        L, _ = s.splat_loss(gn, org, sp, target)   # other scenes' target nodes add a constant
+        g = s.rollout_backward(int(counts[k]))
+        s.close()
+        assert g["d_vel0"].tobytes() == gb["d_vel0"][sl].tobytes(), f"scene {k}: d_vel0 differs"
+        np.testing.assert_allclose(g["d_params"][0], gb["d_params"][k], rtol=1e-10)
+        La += L
+    assert np.isfinite(Lb)
