@@ -377,6 +377,35 @@ typedef struct sph_topology_view {
 
 int sph_rollout_topology(sph_handle *h, uint32_t step, sph_topology_view *v);
 
+/*
+ * Launch shapes.  Each tuned stage of the step launches `block` threads per
+ * block and at most blocks_per_sm x (SM count) blocks, its threads looping
+ * grid-stride over the particles (so blocks_per_sm sets how many particles a
+ * thread covers).  Results do not depend on the shapes.  sph_autotune times
+ * the candidates on the handle's current state (the state is restored after
+ * every trial and at the end), `reps` steps per candidate, stage by stage, and
+ * keeps the fastest; block in {128, 256, 512} (force and energy: 128, 256),
+ * blocks_per_sm in {2, 4, 8, 16, 32}.  Defaults: 256 threads, 8 per SM.
+ */
+#define SPH_TUNE_HASH     0
+#define SPH_TUNE_SCATTER  1
+#define SPH_TUNE_REORDER  2
+#define SPH_TUNE_DENSITY  3
+#define SPH_TUNE_FORCE    4
+#define SPH_TUNE_ENERGY   5
+#define SPH_TUNE_MERGE    6
+#define SPH_TUNE_WRITE    7
+#define SPH_TUNE_STAGES   8
+typedef struct sph_tuning {
+    uint32_t block[SPH_TUNE_STAGES];
+    uint32_t blocks_per_sm[SPH_TUNE_STAGES];   /* 1..64 */
+    float step_ms_before, step_ms_after;       /* sph_autotune: mean step time before / after */
+} sph_tuning;
+
+int sph_set_tuning(sph_handle *h, const sph_tuning *t);
+int sph_get_tuning(const sph_handle *h, sph_tuning *t);
+int sph_autotune(sph_handle *h, uint32_t reps, sph_tuning *out);
+
 /* Human-readable text of the last error on this handle (static storage). */
 const char *sph_last_error(const sph_handle *h);
 

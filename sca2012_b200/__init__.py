@@ -211,6 +211,33 @@ class Solver:
         got = self.read_particles_into(buf.ctypes.data, buf.nbytes)
         return buf[: got * self.record_size].view(particle_dtype(self.dim))
 
+    # -- launch tuning -----------------------------------------------------
+    def autotune(self, reps=3):
+        """Times launch shapes per stage on the current state (restored
+        afterwards) and keeps the fastest; returns the choice and the mean
+        step time before and after."""
+        t = _abi.Tuning()
+        self._check(self._lib.sph_autotune(self._h, int(reps), C.byref(t)), "sph_autotune")
+        return self._tuning_dict(t)
+
+    def get_tuning(self):
+        t = _abi.Tuning()
+        self._check(self._lib.sph_get_tuning(self._h, C.byref(t)), "sph_get_tuning")
+        return self._tuning_dict(t)
+
+    def set_tuning(self, block, blocks_per_sm):
+        t = _abi.Tuning()
+        for k in range(_abi.TUNE_STAGES):
+            t.block[k] = int(block[k])
+            t.blocks_per_sm[k] = int(blocks_per_sm[k])
+        self._check(self._lib.sph_set_tuning(self._h, C.byref(t)), "sph_set_tuning")
+
+    @staticmethod
+    def _tuning_dict(t):
+        return dict(block=list(t.block), blocks_per_sm=list(t.blocks_per_sm),
+                    stages=list(_abi.TUNE_STAGE_NAMES), step_ms_before=t.step_ms_before,
+                    step_ms_after=t.step_ms_after)
+
     # -- differentiable rollout --------------------------------------------
     def rollout_forward(self, nsteps, checkpoint_every):
         """Advances nsteps keeping checkpoints every `checkpoint_every` steps."""

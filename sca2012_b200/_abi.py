@@ -113,6 +113,15 @@ class TopologyView(C.Structure):
                 ("pos", FP), ("vel", FP), ("ev", FP)]
 
 
+TUNE_STAGES = 8
+TUNE_STAGE_NAMES = ("hash", "scatter", "reorder", "density", "force_integrate", "energy_split", "merge", "write")
+
+
+class Tuning(C.Structure):
+    _fields_ = [("block", C.c_uint32 * TUNE_STAGES), ("blocks_per_sm", C.c_uint32 * TUNE_STAGES),
+                ("step_ms_before", C.c_float), ("step_ms_after", C.c_float)]
+
+
 H = C.c_void_p
 DP = C.POINTER(C.c_double)
 
@@ -152,6 +161,9 @@ SIGNATURES = [
     ("sph_splat_loss", C.c_int, [H, C.POINTER(LossGrid), FP, FP, DP]),
     ("sph_rollout_backward", C.c_int, [H, FP, FP, DP, C.c_uint32]),
     ("sph_rollout_topology", C.c_int, [H, C.c_uint32, C.POINTER(TopologyView)]),
+    ("sph_set_tuning", C.c_int, [H, C.POINTER(Tuning)]),
+    ("sph_get_tuning", C.c_int, [H, C.POINTER(Tuning)]),
+    ("sph_autotune", C.c_int, [H, C.c_uint32, C.POINTER(Tuning)]),
     ("sph_last_error", C.c_char_p, [H]),
     ("sph_sort_cells_noalloc", C.c_int, [C.POINTER(Config), C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 using namespace sph;
@@ -63,7 +64,7 @@ struct sph_handle {
     // CUDA graphs of one step, one per buffer parity
     bool use_graph = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    uint32_t graph_grid[2] = {0, 0};
+    uint64_t graph_grid[2] = {0, 0};   // launch_key at capture
     uint32_t graph_launches[2] = {0, 0};
     // batched scenes: device table of 2 float4 per scene (own allocation,
     // replaced by sph_set_scenes)
@@ -73,6 +74,9 @@ struct sph_handle {
     // outside of steps, so a rollout can tell it still describes the state
     Rollout *ro = nullptr;
     uint64_t state_gen = 0;
+    // launch shape per tuned stage (sph_set_tuning / sph_autotune)
+    uint32_t tune_bs[SPH_TUNE_STAGES] = {256, 256, 256, 256, 256, 256, 256, 256};
+    uint32_t tune_bpsm[SPH_TUNE_STAGES] = {8, 8, 8, 8, 8, 8, 8, 8};
 };
 
 namespace {
@@ -131,6 +135,43 @@ uint32_t grid_for(const sph_handle *h, uint32_t work)
     return std::max(1u, std::min(b, cap));
 }
 
+// Grid of a tuned stage: blocks of tune_bs threads, capped at tune_bpsm
+// blocks per SM; the kernels loop grid-stride over the rest.
+uint32_t grid_st(const sph_handle *h, uint32_t work, int stage)
+{
+    const uint32_t bs = h->tune_bs[stage];
+    const uint32_t b = (work + bs - 1) / bs;
+    const uint32_t cap = (uint32_t)h->num_sms * h->tune_bpsm[stage];
+    return std::max(1u, std::min(b, cap));
+}
+
+// Launch key of the step: every stage's grid and block size (a captured
+// graph is valid while it is unchanged).
+uint64_t launch_key(const sph_handle *h)
+{
+    uint64_t k = 1469598103934665603ull;
+    for (int st = 0; st < SPH_TUNE_STAGES; ++st) {
+        const uint32_t work = st == SPH_TUNE_MERGE ? h->ncells : h->n_ub;
+        k = (k ^ grid_st(h, work, st)) * 1099511628211ull;
+        k = (k ^ h->tune_bs[st]) * 1099511628211ull;
+    }
+    return k;
+}
+
+// Instantiates a launch for the stage's block size B (128, 256 or 512; the
+// SWITCH2 kernels hold a 48 KB shared list at 256 threads and stop at 256).
+#define SPH_BS_SWITCH(bs, ...)                                   \
+    switch (bs) {                                                \
+    case 128: { constexpr int B = 128; __VA_ARGS__; } break;     \
+    case 512: { constexpr int B = 512; __VA_ARGS__; } break;     \
+    default: { constexpr int B = 256; __VA_ARGS__; } break;      \
+    }
+#define SPH_BS_SWITCH2(bs, ...)                                  \
+    switch (bs) {                                                \
+    case 128: { constexpr int B = 128; __VA_ARGS__; } break;     \
+    default: { constexpr int B = 256; __VA_ARGS__; } break;      \
+    }
+
 // Exclusive scan of u32 `in` -> `out`; length from len_ptr (device) or len_const.
 void scan_u32(sph_handle *h, const uint32_t *in, uint32_t *out, const uint32_t *len_ptr, uint32_t len_const,
               uint32_t *grand, int total_at_len, uint32_t *list)
@@ -170,23 +211,27 @@ template <int DIM> int run_step(sph_handle *h)
     CanonPtrs in = h->buf[p], out = h->buf[p ^ 1];
     h->w.pos_comp = c.compensated_positions ? 1u : 0u;
     WorkPtrs w = h->w;
-    const uint32_t G = grid_for(h, h->n_ub);
     cudaStream_t s = h->stream;
     h->nstages = 0;
     if (h->profiling) cudaEventRecord(h->ev[0], s);
 
     cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, s);
-    k_hash<DIM><<<G, kThreads, 0, s>>>(c, cin, in, w);
+    const uint32_t nub = h->n_ub;
+    SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_HASH],
+                  k_hash<DIM, B><<<grid_st(h, nub, SPH_TUNE_HASH), B, 0, s>>>(c, cin, in, w));
     stage(h, "hash");
     scan_u32(h, w.cell_count, w.cell_off, nullptr, h->ncells, h->scan_grand, 1, nullptr);
     stage(h, "scan_cells");
-    k_scatter<<<G, kThreads, 0, s>>>(cin, w);
+    SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_SCATTER], k_scatter<B><<<grid_st(h, nub, SPH_TUNE_SCATTER), B, 0, s>>>(cin, w));
     stage(h, "scatter");
-    k_reorder<<<G, kThreads, 0, s>>>(cin, in, w);
+    SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_REORDER],
+                  k_reorder<B><<<grid_st(h, nub, SPH_TUNE_REORDER), B, 0, s>>>(cin, in, w));
     stage(h, "reorder");
-    k_density<DIM><<<G, kThreads, 0, s>>>(c, cin, w);
+    SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_DENSITY],
+                  k_density<DIM, B><<<grid_st(h, nub, SPH_TUNE_DENSITY), B, 0, s>>>(c, cin, w));
     stage(h, "density");
-    k_force_integrate<DIM><<<G, kThreads, 0, s>>>(c, cin, w);
+    SPH_BS_SWITCH2(h->tune_bs[SPH_TUNE_FORCE],
+                   k_force_integrate<DIM, B><<<grid_st(h, nub, SPH_TUNE_FORCE), B, 0, s>>>(c, cin, w));
     stage(h, "force_integrate");
     // density grid + surface mid-step: stale cell lists, integrated positions
     // (SPH-3D-2/sph_system.cpp:336-362)
@@ -198,22 +243,26 @@ template <int DIM> int run_step(sph_handle *h)
         h->grid_valid = true;
         stage(h, "surface");
     }
-    k_energy_split<DIM><<<G, kThreads, 0, s>>>(c, cin, in, w, h->debug ? 1 : 0);
+    SPH_BS_SWITCH2(h->tune_bs[SPH_TUNE_ENERGY],
+                   k_energy_split<DIM, B><<<grid_st(h, nub, SPH_TUNE_ENERGY), B, 0, s>>>(c, cin, in, w,
+                                                                                       h->debug ? 1 : 0));
     stage(h, "energy_split");
     h->last_launches += 6;
     scan_u32(h, w.split_c, w.split_rank, &cin->n, 0, &cin->n_split, 0, w.split_list);
     k_split_guard<<<1, 1, 0, s>>>(c, cin, h->cap);
     h->last_launches += 1;
     stage(h, "scan_split");
-    if (c.use_merge) {
-        const uint32_t GM = grid_for(h, h->ncells);   // a warp scans 32 cells at a time
-        k_merge<DIM><<<GM, kThreads, 0, s>>>(c, cin, in, w, h->ncells, h->cap);
+    if (c.use_merge) {   // one lane per cell, a warp scans 32 cells at a time
+        SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_MERGE],
+                      k_merge<DIM, B><<<grid_st(h, h->ncells, SPH_TUNE_MERGE), B, 0, s>>>(c, cin, in, w, h->ncells,
+                                                                                          h->cap));
         h->last_launches += 1;
         stage(h, "merge");
     }
     scan_u32(h, w.removed_c, w.removed_rank, &cin->n, 0, &cin->n_removed, 0, nullptr);
     stage(h, "scan_removed");
-    k_write<DIM><<<G, kThreads, 0, s>>>(c, cin, cout, out, w);
+    SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_WRITE],
+                  k_write<DIM, B><<<grid_st(h, nub, SPH_TUNE_WRITE), B, 0, s>>>(c, cin, cout, out, w));
     h->last_launches += 1;
     stage(h, "write");
     h->cur = p ^ 1;
@@ -506,7 +555,7 @@ static int capture_step(sph_handle *h)
     e = cudaGraphInstantiate(&h->graph[p], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_check(h, "cudaGraphInstantiate");
-    h->graph_grid[p] = grid_for(h, h->n_ub);
+    h->graph_grid[p] = launch_key(h);
     return SPH_OK;
 }
 
@@ -527,7 +576,7 @@ int sph_step(sph_handle *h, int nsteps)
         int rc;
         if (h->use_graph && !h->profiling && !surface_due) {
             const int p = h->cur;
-            if (!h->graph[p] || h->graph_grid[p] != grid_for(h, h->n_ub)) {
+            if (!h->graph[p] || h->graph_grid[p] != launch_key(h)) {
                 rc = capture_step(h);
                 if (rc) return rc;
             }
@@ -944,5 +993,163 @@ int sph_surface_from_grid(sph_handle *h, const float *dens, const float *normal,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- launch tuning
+namespace {
+
+bool tune_valid(int st, uint32_t bs, uint32_t bpsm)
+{
+    const bool big_ok = st != SPH_TUNE_FORCE && st != SPH_TUNE_ENERGY;
+    return (bs == 128 || bs == 256 || (bs == 512 && big_ok)) && bpsm >= 1 && bpsm <= 64;
+}
+
+const char *const kTuneStageName[SPH_TUNE_STAGES] = {"hash", "scatter", "reorder", "density",
+                                                     "force_integrate", "energy_split", "merge", "write"};
+
+}  // namespace
+
+int sph_set_tuning(sph_handle *h, const sph_tuning *t)
+{
+    if (!h || !t) return SPH_ERR_INVALID;
+    for (int st = 0; st < SPH_TUNE_STAGES; ++st)
+        if (!tune_valid(st, t->block[st], t->blocks_per_sm[st])) {
+            h->err = std::string("sph_set_tuning: unsupported shape for stage ") + kTuneStageName[st];
+            return SPH_ERR_INVALID;
+        }
+    for (int st = 0; st < SPH_TUNE_STAGES; ++st) {
+        h->tune_bs[st] = t->block[st];
+        h->tune_bpsm[st] = t->blocks_per_sm[st];
+    }
+    drop_graphs(h);
+    return SPH_OK;
+}
+
+int sph_get_tuning(const sph_handle *h, sph_tuning *t)
+{
+    if (!h || !t) return SPH_ERR_INVALID;
+    for (int st = 0; st < SPH_TUNE_STAGES; ++st) {
+        t->block[st] = h->tune_bs[st];
+        t->blocks_per_sm[st] = h->tune_bpsm[st];
+    }
+    t->step_ms_before = t->step_ms_after = 0.0f;
+    return SPH_OK;
+}
+
+int sph_autotune(sph_handle *h, uint32_t reps, sph_tuning *out)
+{
+    if (!h || reps == 0) return SPH_ERR_INVALID;
+    sph_readback_wait(h);
+    const uint32_t n = read_n(h);
+    if (n == 0) { h->err = "sph_autotune: no particles"; return SPH_ERR_INVALID; }
+    // the state every trial starts from
+    CanonPtrs save{};
+    std::vector<void *> tmp;
+    auto talloc = [&](auto **p, size_t count) {
+        void *q = nullptr;
+        if (cudaMalloc(&q, sizeof(**p) * count) != cudaSuccess) return 1;
+        tmp.push_back(q);
+        *p = (std::remove_reference_t<decltype(*p)>)q;
+        return 0;
+    };
+    int bad = talloc(&save.pos, n) | talloc(&save.vel, n) | talloc(&save.ev, n) | talloc(&save.acc, n) |
+              talloc(&save.dens, n) | talloc(&save.press, n) | talloc(&save.energy, n) |
+              talloc(&save.surface, n) | talloc(&save.interior, n) | talloc(&save.scene, n) |
+              talloc(&save.pos_lo, n);
+    if (bad) {
+        cudaGetLastError();
+        for (void *p : tmp) cudaFree(p);
+        h->err = "sph_autotune: out of device memory for the saved state";
+        return SPH_ERR_CUDA;
+    }
+    auto copy = [&](const CanonPtrs &d, const CanonPtrs &src) {
+        auto c1 = [&](void *dd, const void *ss, size_t bytes) {
+            cudaMemcpyAsync(dd, ss, bytes, cudaMemcpyDeviceToDevice, h->stream);
+        };
+        c1(d.pos, src.pos, 16ull * n); c1(d.vel, src.vel, 16ull * n); c1(d.ev, src.ev, 16ull * n);
+        c1(d.acc, src.acc, 16ull * n); c1(d.dens, src.dens, 4ull * n); c1(d.press, src.press, 4ull * n);
+        c1(d.energy, src.energy, 4ull * n); c1(d.surface, src.surface, 4ull * n);
+        c1(d.interior, src.interior, 4ull * n); c1(d.scene, src.scene, 4ull * n);
+        c1(d.pos_lo, src.pos_lo, 16ull * n);
+    };
+    copy(save, h->buf[h->cur]);
+    const int cur0 = h->cur;
+    const uint64_t step0 = h->step_index;
+    const bool prof0 = h->profiling;
+    const bool graph0 = h->use_graph;
+    h->use_graph = false;
+    drop_graphs(h);
+    sph_set_profiling(h, 1);
+    auto restore = [&]() {
+        h->cur = cur0;
+        copy(h->buf[h->cur], save);
+        Counters c0;
+        std::memset(&c0, 0, sizeof(c0));
+        c0.n = n;
+        cudaMemcpyAsync(&h->cnt[h->cur], &c0, sizeof(Counters), cudaMemcpyHostToDevice, h->stream);
+        h->n_ub = n;
+        h->step_index = step0;
+    };
+    // per-stage and whole-step device time over `reps` steps from the saved state
+    std::vector<float> stage_ms(SPH_TUNE_STAGES);
+    float step_ms = 0.0f;
+    auto trial = [&]() -> int {
+        restore();
+        std::fill(stage_ms.begin(), stage_ms.end(), 0.0f);
+        step_ms = 0.0f;
+        for (uint32_t r = 0; r < reps; ++r) {
+            int rc = h->cfg.dim == 3 ? run_step<3>(h) : run_step<2>(h);
+            if (rc) return rc;
+            float ms[sph_handle::kMaxStages];
+            const char *names[sph_handle::kMaxStages];
+            int cnt = 0;
+            if ((rc = sph_stage_times(h, ms, names, sph_handle::kMaxStages, &cnt))) return rc;
+            for (int q = 0; q < cnt; ++q) {
+                step_ms += ms[q];
+                for (int st = 0; st < SPH_TUNE_STAGES; ++st)
+                    if (!std::strcmp(names[q], kTuneStageName[st])) stage_ms[st] += ms[q];
+            }
+        }
+        return SPH_OK;
+    };
+    int rc = trial();
+    const float before = step_ms / reps;
+    static const uint32_t kBs[3] = {128, 256, 512};
+    static const uint32_t kBpsm[5] = {2, 4, 8, 16, 32};
+    for (int st = 0; st < SPH_TUNE_STAGES && !rc; ++st) {
+        if (st == SPH_TUNE_MERGE && !h->cfg.use_merge) continue;
+        uint32_t best_bs = h->tune_bs[st], best_bp = h->tune_bpsm[st];
+        if ((rc = trial())) break;
+        float best = stage_ms[st];
+        for (uint32_t bs : kBs)
+            for (uint32_t bp : kBpsm) {
+                if (!tune_valid(st, bs, bp) || (bs == best_bs && bp == best_bp)) continue;
+                h->tune_bs[st] = bs;
+                h->tune_bpsm[st] = bp;
+                if ((rc = trial())) break;
+                if (stage_ms[st] < best * 0.98f) {   // keep a change only for a clear gain
+                    best = stage_ms[st];
+                    best_bs = bs;
+                    best_bp = bp;
+                }
+            }
+        h->tune_bs[st] = best_bs;
+        h->tune_bpsm[st] = best_bp;
+    }
+    float after = before;
+    if (!rc && !(rc = trial())) after = step_ms / reps;
+    restore();
+    cudaStreamSynchronize(h->stream);
+    for (void *p : tmp) cudaFree(p);
+    sph_set_profiling(h, prof0 ? 1 : 0);
+    h->use_graph = graph0;
+    h->have_step = false;
+    if (rc) return rc;
+    if (out) {
+        sph_get_tuning(h, out);
+        out->step_ms_before = before;
+        out->step_ms_after = after;
+    }
+    return cuda_check(h, "sph_autotune");
+}
 
 #include "sph_rollout_impl.cuh"

@@ -173,8 +173,8 @@ __device__ __forceinline__ int row_range_pruned(const sph_config &c, const uint3
 }
 
 // ------------------------------------------------------------ 1. hash
-template <int DIM>
-__global__ void __launch_bounds__(kThreads) k_hash(sph_config c, const Counters *__restrict__ cnt,
+template <int DIM, int BS = kThreads>
+__global__ void __launch_bounds__(BS) k_hash(sph_config c, const Counters *__restrict__ cnt,
                                                   CanonPtrs st, WorkPtrs w)
 {
     const uint32_t n = cnt->n;
@@ -187,7 +187,8 @@ __global__ void __launch_bounds__(kThreads) k_hash(sph_config c, const Counters 
 }
 
 // ------------------------------------------------------------ 3. scatter
-__global__ void __launch_bounds__(kThreads) k_scatter(const Counters *__restrict__ cnt, WorkPtrs w)
+template <int BS = kThreads>
+__global__ void __launch_bounds__(BS) k_scatter(const Counters *__restrict__ cnt, WorkPtrs w)
 {
     const uint32_t n = cnt->n;
     for (uint32_t i = grid_stride_start(); i < n; i += grid_stride())
@@ -199,7 +200,8 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const Counters *__restrict
 // keys in ascending particle index, as thrust's radix sort_by_key leaves
 // them, SPH-3D-2/sph_system.cu:119-129) is restored by ranking each particle
 // among its cell's members.  Then the state is gathered into key order.
-__global__ void __launch_bounds__(kThreads) k_reorder(const Counters *__restrict__ cnt, CanonPtrs st, WorkPtrs w)
+template <int BS = kThreads>
+__global__ void __launch_bounds__(BS) k_reorder(const Counters *__restrict__ cnt, CanonPtrs st, WorkPtrs w)
 {
     const uint32_t n = cnt->n;
     for (uint32_t s = grid_stride_start(); s < n; s += grid_stride()) {
@@ -232,8 +234,8 @@ constexpr uint32_t kListLen = 48;   // 48 x 256 x 4 B = 48 KB of shared memory p
 // ------------------------------------------------------------ 5. density
 // rho_i = m_i poly6_i h_i^6 + sum_{j != i, skip <= r^2 < h_i^2} m_j poly6_i (h_i^2 - r^2)^3
 // p_i = k ((rho_i / rho0)^3 - 1)         (SPH-3D-2/sph_system.cu:338-677)
-template <int DIM>
-__global__ void __launch_bounds__(kThreads) k_density(sph_config c, const Counters *__restrict__ cnt, WorkPtrs w)
+template <int DIM, int BS = kThreads>
+__global__ void __launch_bounds__(BS) k_density(sph_config c, const Counters *__restrict__ cnt, WorkPtrs w)
 {
     const uint32_t n = cnt->n;
     for (uint32_t s = grid_stride_start(); s < n; s += grid_stride()) {
@@ -290,11 +292,11 @@ __global__ void __launch_bounds__(kThreads) k_density(sph_config c, const Counte
 // 2D SPH-2D/sph_system.cu:462-790), then the integrator and walls
 // (SPH-3D-2/sph_system.cu:204-322, SPH-2D/sph_system.cu:198-252).  The
 // integrated state goes to the *_n arrays so the loop never sees it.
-template <int DIM>
-__global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, const Counters *__restrict__ cnt,
+template <int DIM, int BS = kThreads>
+__global__ void __launch_bounds__(BS) k_force_integrate(sph_config c, const Counters *__restrict__ cnt,
                                                               WorkPtrs w)
 {
-    __shared__ uint32_t nlist[kListLen][kThreads];
+    __shared__ uint32_t nlist[kListLen][BS];
     const uint32_t n = cnt->n;
     for (uint32_t s = grid_stride_start(); s < n; s += grid_stride()) {
         const float4 pi = w.spos[s];
@@ -324,7 +326,7 @@ __global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, cons
         // phase B: the interaction math over the listed neighbours
         auto flush = [&]() {
             for (uint32_t kk = 0; kk < cntl; ++kk) {
-                const uint32_t t = my_list[kk * kThreads];
+                const uint32_t t = my_list[kk * BS];
                 const float4 pj = w.spos[t];
                 float rx, ry, rz;
                 const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
@@ -364,7 +366,7 @@ __global__ void __launch_bounds__(kThreads) k_force_integrate(sph_config c, cons
             const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
             const float cut = pj.w == 1.0f ? cut0 : cut1;
             if (t != s && r2 < cut && !(r2 < 0.0001f)) {
-                my_list[cntl * kThreads] = t;
+                my_list[cntl * BS] = t;
                 if (++cntl == kListLen) flush();
             }
         };
@@ -498,11 +500,11 @@ __device__ __forceinline__ float wavelet(float x, float amp)
     return amp * (x2 * 0.25f - 1.0f) * exp2f(-x2 * 0.125f * 1.44269476f);
 }
 
-template <int DIM>
-__global__ void __launch_bounds__(kThreads) k_energy_split(sph_config c, Counters *__restrict__ cnt,
+template <int DIM, int BS = kThreads>
+__global__ void __launch_bounds__(BS) k_energy_split(sph_config c, Counters *__restrict__ cnt,
                                                            CanonPtrs st, WorkPtrs w, int want_tv)
 {
-    __shared__ uint32_t nlist[kListLen][kThreads];
+    __shared__ uint32_t nlist[kListLen][BS];
     const uint32_t n = cnt->n;
     // 2/(PI^0.25 * sqrt(3 sigma)) with PI = 3.141592f, sigma = 2
     const float amp = 2.0f / (powf(3.141592f, 0.25f) * sqrtf(6.0f));
@@ -520,7 +522,7 @@ __global__ void __launch_bounds__(kThreads) k_energy_split(sph_config c, Counter
         // phase B: the wavelet transform over the listed neighbours
         auto flush = [&]() {
             for (uint32_t kk = 0; kk < cntl; ++kk) {
-                const uint32_t t = my_list[kk * kThreads];
+                const uint32_t t = my_list[kk * BS];
                 const float4 pj = w.spos_n[t];
                 const float4 vj = w.svel_n[t];
                 float rx, ry, rz;
@@ -541,7 +543,7 @@ __global__ void __launch_bounds__(kThreads) k_energy_split(sph_config c, Counter
             float rx, ry, rz;
             const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
             if (t != s && r2 < h2 && !(r2 < skip)) {
-                my_list[cntl * kThreads] = t;
+                my_list[cntl * BS] = t;
                 if (++cntl == kListLen) flush();
             }
         };
@@ -670,11 +672,11 @@ __device__ __forceinline__ void merge_group(const sph_config &c, const WorkPtrs 
     }
 }
 
-template <int DIM>
-__global__ void __launch_bounds__(kThreads) k_merge(sph_config c, const Counters *__restrict__ cnt,
+template <int DIM, int BS = kThreads>
+__global__ void __launch_bounds__(BS) k_merge(sph_config c, const Counters *__restrict__ cnt,
                                                    CanonPtrs st, WorkPtrs w, uint32_t ncells, uint32_t cap)
 {
-    __shared__ uint32_t list[kThreads / 32][kMergeListMax];
+    __shared__ uint32_t list[BS / 32][kMergeListMax];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
     const uint32_t n = cnt->n;
@@ -750,8 +752,8 @@ __global__ void __launch_bounds__(kThreads) k_merge(sph_config c, const Counters
 // [surviving particles in index order][children in split order][removed].
 // Children follow adaptive_particle_kernel (:1576-1615; 3D-4 :1583-1656;
 // 2D :1133-1160).  Writes the other canonical buffer.
-template <int DIM>
-__global__ void __launch_bounds__(kThreads) k_write(sph_config c, const Counters *__restrict__ cnt,
+template <int DIM, int BS = kThreads>
+__global__ void __launch_bounds__(BS) k_write(sph_config c, const Counters *__restrict__ cnt,
                                                    Counters *__restrict__ cnt_next, CanonPtrs out, WorkPtrs w)
 {
     const uint32_t n = cnt->n;
