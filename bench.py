@@ -65,6 +65,7 @@ def parse():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--cpu-sample-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     p.add_argument("--batch-scenes", type=int, default=256, help="0 skips the batched-scenes comparison")
     p.add_argument("--batch-steps", type=int, default=20)
     p.add_argument("--rollout-steps", type=int, default=200, help="0 skips the differentiable-rollout timing")
@@ -182,6 +183,8 @@ def run_ours(args, rank, world, local_rank):
         s.step(1)
     if s.sync_status():
         raise RuntimeError("solver reported an error during warm-up")
+    # launch shapes picked by the autotuner on this state (restored afterwards)
+    tuning = None if args.no_autotune else s.autotune(reps=3)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     counts = []
     launches = 0
@@ -336,6 +339,7 @@ def run_ours(args, rank, world, local_rank):
                          "launch_ms": stage_avg[top], "peak_source": peak_src,
                          "note": "neighbour loops are FP32-issue bound: the HBM fraction is low by design"},
             "stages_ms": stage_avg,
+            "tuning": tuning,
             "ref_3d2_default_scene": small,
             "batched_scenes": batched,
             "rollout": roll,
