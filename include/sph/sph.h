@@ -377,6 +377,12 @@ typedef struct sph_topology_view {
 
 int sph_rollout_topology(sph_handle *h, uint32_t step, sph_topology_view *v);
 
+/* Conserved quantities of the current state, summed in FP64 on the device
+ * (deterministic order): out[0] total mass, out[1..3] momentum, out[4]
+ * kinetic energy, out[5] gravitational potential energy -m g.x, out[6] their
+ * sum.  Synchronous. */
+int sph_conserved(sph_handle *h, double out[7]);
+
 /*
  * Launch shapes.  Each tuned stage of the step launches `block` threads per
  * block and at most blocks_per_sm x (SM count) blocks, its threads looping

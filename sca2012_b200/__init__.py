@@ -211,6 +211,12 @@ class Solver:
         got = self.read_particles_into(buf.ctypes.data, buf.nbytes)
         return buf[: got * self.record_size].view(particle_dtype(self.dim))
 
+    def conserved(self):
+        """FP64 device sums: mass, momentum (3), kinetic, potential, total energy."""
+        out = np.zeros(7, np.float64)
+        self._check(self._lib.sph_conserved(self._h, out.ctypes.data_as(_abi.DP)), "sph_conserved")
+        return dict(mass=out[0], momentum=out[1:4].copy(), kinetic=out[4], potential=out[5], energy=out[6])
+
     # -- launch tuning -----------------------------------------------------
     def autotune(self, reps=3):
         """Times launch shapes per stage on the current state (restored

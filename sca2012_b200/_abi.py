@@ -161,6 +161,7 @@ SIGNATURES = [
     ("sph_splat_loss", C.c_int, [H, C.POINTER(LossGrid), FP, FP, DP]),
     ("sph_rollout_backward", C.c_int, [H, FP, FP, DP, C.c_uint32]),
     ("sph_rollout_topology", C.c_int, [H, C.c_uint32, C.POINTER(TopologyView)]),
+    ("sph_conserved", C.c_int, [H, DP]),
     ("sph_set_tuning", C.c_int, [H, C.POINTER(Tuning)]),
     ("sph_get_tuning", C.c_int, [H, C.POINTER(Tuning)]),
     ("sph_autotune", C.c_int, [H, C.c_uint32, C.POINTER(Tuning)]),

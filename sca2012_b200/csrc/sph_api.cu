@@ -75,6 +75,7 @@ struct sph_handle {
     Rollout *ro = nullptr;
     uint64_t state_gen = 0;
     // launch shape per tuned stage (sph_set_tuning / sph_autotune)
+    double *cons = nullptr;   // conserved-quantity partial sums (allocated on first use)
     uint32_t tune_bs[SPH_TUNE_STAGES] = {256, 256, 256, 256, 256, 256, 256, 256};
     uint32_t tune_bpsm[SPH_TUNE_STAGES] = {8, 8, 8, 8, 8, 8, 8, 8};
 };
@@ -405,6 +406,7 @@ int sph_destroy(sph_handle *h)
     rollout_free(h->ro);
     for (void *p : h->allocs) cudaFree(p);
     if (h->scene_tab) cudaFree(h->scene_tab);
+    if (h->cons) cudaFree(h->cons);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return SPH_OK;
@@ -690,6 +692,31 @@ int sph_sync(sph_handle *h)
             }
     }
     return SPH_OK;
+}
+
+int sph_conserved(sph_handle *h, double *out)
+{
+    if (!h || !out) return SPH_ERR_INVALID;
+    const uint32_t G = grid_for(h, h->n_ub);
+    if (!h->cons) {
+        if (cudaMalloc(&h->cons, sizeof(double) * ((size_t)h->num_sms * 8u + 1) * kConservedTerms) != cudaSuccess) {
+            cudaGetLastError();
+            h->cons = nullptr;
+            h->err = "sph_conserved: out of device memory";
+            return SPH_ERR_CUDA;
+        }
+    }
+    double *fin = h->cons + (size_t)h->num_sms * 8u * kConservedTerms;
+    cudaStream_t s = h->stream;
+    if (h->cfg.dim == 3) k_conserved<3><<<G, kThreads, 0, s>>>(h->cfg, h->cnt + h->cur, h->buf[h->cur], h->cons);
+    else k_conserved<2><<<G, kThreads, 0, s>>>(h->cfg, h->cnt + h->cur, h->buf[h->cur], h->cons);
+    k_conserved_final<<<1, 32, 0, s>>>(h->cons, G, fin);
+    double v[kConservedTerms];
+    cudaMemcpyAsync(v, fin, sizeof(v), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    for (int k = 0; k < kConservedTerms; ++k) out[k] = v[k];
+    out[6] = v[4] + v[5];
+    return cuda_check(h, "sph_conserved");
 }
 
 int sph_get_num_particles(sph_handle *h, uint32_t *n)

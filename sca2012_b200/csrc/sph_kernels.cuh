@@ -909,6 +909,52 @@ __global__ void __launch_bounds__(kThreads) k_from_aos(uint32_t n, CanonPtrs st,
     }
 }
 
+// ------------------------------------------------------------ conserved quantities
+// Per-block FP64 partial sums of mass, momentum (3), kinetic energy and
+// gravitational potential energy (-m g.x) over the canonical state; a second
+// single-block pass adds the partials in block order (deterministic).
+constexpr int kConservedTerms = 6;
+
+template <int DIM>
+__global__ void __launch_bounds__(kThreads) k_conserved(sph_config c, const Counters *__restrict__ cnt, CanonPtrs st,
+                                                        double *partial)
+{
+    const uint32_t n = cnt->n;
+    double acc[kConservedTerms] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) {
+        const float4 p = st.pos[i], v = st.vel[i];
+        const double m = c.mass[lv(p.w)];
+        const double vx = v.x, vy = v.y, vz = DIM == 3 ? v.z : 0.0;
+        acc[0] += m;
+        acc[1] += m * vx; acc[2] += m * vy; acc[3] += m * vz;
+        acc[4] += 0.5 * m * (vx * vx + vy * vy + vz * vz);
+        acc[5] -= m * ((double)c.gravity[0] * p.x + (double)c.gravity[1] * p.y +
+                       (DIM == 3 ? (double)c.gravity[2] * p.z : 0.0));
+    }
+    __shared__ double red[kThreads / 32][kConservedTerms];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int k = 0; k < kConservedTerms; ++k) {
+        double x = acc[k];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) red[wid][k] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < kConservedTerms) {
+        double x = 0.0;
+        for (int q = 0; q < kThreads / 32; ++q) x += red[q][threadIdx.x];
+        partial[(size_t)blockIdx.x * kConservedTerms + threadIdx.x] = x;
+    }
+}
+
+__global__ void k_conserved_final(const double *partial, uint32_t blocks, double *out)
+{
+    if (threadIdx.x < kConservedTerms) {
+        double x = 0.0;
+        for (uint32_t b = 0; b < blocks; ++b) x += partial[(size_t)b * kConservedTerms + threadIdx.x];
+        out[threadIdx.x] = x;
+    }
+}
+
 // ------------------------------------------------------------ debug helpers
 __global__ void k_cell_ranges(const uint32_t *__restrict__ off, uint32_t ncells, uint32_t *start, uint32_t *end)
 {
