@@ -161,6 +161,20 @@ def cpu_baseline(cfg, pos, vel, lvl, steps, threads=None):
 
 
 # ----------------------------------------------------------------- our arm
+def reduce_over_ranks(t_ms, units, dist, device):
+    """Whole-job timing of independent replicas: the slowest rank's time and
+    the units all ranks processed (every rank calls it, in the same order)."""
+    if not dist:
+        return t_ms, units
+    import torch
+    import torch.distributed as tdist
+    t = torch.tensor([t_ms], device=device, dtype=torch.float64)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    u = torch.tensor([units], device=device, dtype=torch.float64)
+    tdist.all_reduce(u)
+    return float(t.item()), float(u.item())
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import sca2012_b200 as sph
@@ -212,12 +226,7 @@ def run_ours(args, rank, world, local_rank):
     times = [a.elapsed_time(b) for a, b in ev]
     t_ms = float(sum(times))
     ps = float(sum(counts))
-    if dist:
-        t = torch.tensor([t_ms], device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        p = torch.tensor([ps], device="cuda", dtype=torch.float64)
-        tdist.all_reduce(p)
-        t_ms, ps = float(t.item()), float(p.item())
+    t_ms, ps = reduce_over_ranks(t_ms, ps, dist, "cuda")
     value = ps / (t_ms * 1e-3)
 
     # --- per-stage durations (separate profiled steps, same stream)
@@ -281,12 +290,7 @@ def run_ours(args, rank, world, local_rank):
         h2d += n_cur * rec
         d2h += n_next * rec + 4
         n_cur = n_next
-    if dist:
-        t = torch.tensor([e2e_t], device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        p = torch.tensor([e2e_ps], device="cuda", dtype=torch.float64)
-        tdist.all_reduce(p)
-        e2e_t, e2e_ps = float(t.item()), float(p.item())
+    e2e_t, e2e_ps = reduce_over_ranks(e2e_t, e2e_ps, dist, "cuda")
     e2e_value = e2e_ps / (e2e_t * 1e-3)
     status |= s.sync_status()
     s.close()
@@ -379,6 +383,13 @@ def batched_scenes(args):
         base.use_split = base.use_merge = 1
         batches.append(sc.batch_scenes(base, half, seed=seed))
 
+    def timed_call(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
     def timed(solvers, k, per_scene_sync=False):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -403,6 +414,17 @@ def batched_scenes(args):
     timed(bs, 3)
     t_batched = timed(bs, steps)
     status = 0
+    # the adjoint of the last 50 steps, batched: checkpointed forward, a
+    # density-grid loss over every scene (nodes at cell centres), backward
+    t_fwd = t_bwd = 0.0
+    adj_steps = 50
+    for h, (cfg, boxes, *_rest) in zip(bs, batches):
+        gn = tuple(int(cfg.ncell[a]) for a in range(3))
+        org = tuple(0.5 * float(cfg.cell_size) for _ in range(3))
+        n_start = h.num_particles()
+        t_fwd += timed_call(lambda: h.rollout_forward(adj_steps, 10))
+        h.splat_loss(gn, org, float(cfg.cell_size), np.zeros(int(np.prod(gn)), np.float32))
+        t_bwd += timed_call(lambda: h.rollout_backward(n_start, nscenes=len(boxes)))
     for h in bs:
         status |= h.sync_status()
         h.close()
@@ -436,6 +458,10 @@ def batched_scenes(args):
             "concurrent_streams_scene_steps_per_s": v_c,
             "batched_vs_sequential": v_b / v_s, "batched_vs_concurrent_streams": v_b / v_c,
             "batched_ms_per_step": t_batched / steps * 1e3, "status": status,
+            "adjoint_last_50": {"forward_ms_per_step": t_fwd / adj_steps * 1e3,
+                                "backward_ms_per_step": t_bwd / adj_steps * 1e3,
+                                "backward_vs_forward": t_bwd / t_fwd,
+                                "loss": "mean squared density grid (nodes at cell centres), per-scene gradients"},
             "timing": "wall clock around synchronised step loops"}
 
 
