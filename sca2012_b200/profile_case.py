@@ -1,12 +1,16 @@
 """Fixed workload runner for profiling the step's kernels under ncu.
 
     python -m sca2012_b200.profile_case [--particles N] [--steps K] [--adaptive 0|1]
+                                        [--block B0,..,B7 --bpsm P0,..,P7]
 
 Runs the four-way dam-break workload (the bench workload, optionally with the
 block shrunk to about N particles) for K steps on cuda:0 and exits 0.  Every
 step issues each kernel once, so `ncu -k regex:<kernel> -s <K-1> -c 1`
 captures the last step's launch.  Device memory stays near 450 bytes per
-particle of capacity (capacity = 1.5 x the initial count).
+particle of capacity (capacity = 1.5 x the initial count).  --block/--bpsm
+set the launch shapes per tuned stage (the order of sph_tuning: hash,
+scatter, reorder, density, force, energy, merge, write), e.g. the ones the
+benchmark's autotuner reported.
 """
 import argparse
 import sys
@@ -22,6 +26,8 @@ def main():
     ap.add_argument("--particles", type=int, default=0, help="0 = full 1,114,112-particle workload")
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--adaptive", type=int, default=1)
+    ap.add_argument("--block", default="")
+    ap.add_argument("--bpsm", default="")
     a = ap.parse_args()
     cfg = sph.preset(sph.PRESET_DAM_3D4)
     pos, vel, lvl = scenes.dam_3d4(cfg)
@@ -33,6 +39,11 @@ def main():
     cfg.use_merge = a.adaptive
     cfg.max_particle = int(len(pos) * 1.5) + 1024
     s = sph.Solver(cfg)
+    if a.block or a.bpsm:
+        t = s.get_tuning()
+        block = [int(x) for x in a.block.split(",")] if a.block else t["block"]
+        bpsm = [int(x) for x in a.bpsm.split(",")] if a.bpsm else t["blocks_per_sm"]
+        s.set_tuning(block, bpsm)
     s.set_state(dict(pos=pos, vel=vel, level=lvl))
     s.step(a.steps)
     rc = s.sync_status()
