@@ -421,6 +421,7 @@ def batched_scenes(args):
     for h, (cfg, boxes, *_rest) in zip(bs, batches):
         gn = tuple(int(cfg.ncell[a]) for a in range(3))
         org = tuple(0.5 * float(cfg.cell_size) for _ in range(3))
+        h.rollout_forward(adj_steps, 10)   # allocates checkpoints and tape (untimed)
         n_start = h.num_particles()
         t_fwd += timed_call(lambda: h.rollout_forward(adj_steps, 10))
         h.splat_loss(gn, org, float(cfg.cell_size), np.zeros(int(np.prod(gn)), np.float32))
@@ -461,6 +462,7 @@ def batched_scenes(args):
             "adjoint_last_50": {"forward_ms_per_step": t_fwd / adj_steps * 1e3,
                                 "backward_ms_per_step": t_bwd / adj_steps * 1e3,
                                 "backward_vs_forward": t_bwd / t_fwd,
+                                "backward_vs_plain_batched_step": (t_bwd / adj_steps) / (t_batched / steps),
                                 "loss": "mean squared density grid (nodes at cell centres), per-scene gradients"},
             "timing": "wall clock around synchronised step loops"}
 
