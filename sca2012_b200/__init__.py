@@ -231,16 +231,17 @@ class Solver:
         self._check(self._lib.sph_get_tuning(self._h, C.byref(t)), "sph_get_tuning")
         return self._tuning_dict(t)
 
-    def set_tuning(self, block, blocks_per_sm):
+    def set_tuning(self, block, blocks_per_sm, reg_cap=None):
         t = _abi.Tuning()
         for k in range(_abi.TUNE_STAGES):
             t.block[k] = int(block[k])
             t.blocks_per_sm[k] = int(blocks_per_sm[k])
+            t.reg_cap[k] = int(reg_cap[k]) if reg_cap is not None else 0
         self._check(self._lib.sph_set_tuning(self._h, C.byref(t)), "sph_set_tuning")
 
     @staticmethod
     def _tuning_dict(t):
-        return dict(block=list(t.block), blocks_per_sm=list(t.blocks_per_sm),
+        return dict(block=list(t.block), blocks_per_sm=list(t.blocks_per_sm), reg_cap=list(t.reg_cap),
                     stages=list(_abi.TUNE_STAGE_NAMES), step_ms_before=t.step_ms_before,
                     step_ms_after=t.step_ms_after)
 

@@ -119,7 +119,7 @@ TUNE_STAGE_NAMES = ("hash", "scatter", "reorder", "density", "force_integrate", 
 
 class Tuning(C.Structure):
     _fields_ = [("block", C.c_uint32 * TUNE_STAGES), ("blocks_per_sm", C.c_uint32 * TUNE_STAGES),
-                ("step_ms_before", C.c_float), ("step_ms_after", C.c_float)]
+                ("reg_cap", C.c_uint32 * TUNE_STAGES), ("step_ms_before", C.c_float), ("step_ms_after", C.c_float)]
 
 
 H = C.c_void_p

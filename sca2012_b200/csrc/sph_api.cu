@@ -78,6 +78,7 @@ struct sph_handle {
     double *cons = nullptr;   // conserved-quantity partial sums (allocated on first use)
     uint32_t tune_bs[SPH_TUNE_STAGES] = {256, 256, 256, 256, 256, 256, 256, 256};
     uint32_t tune_bpsm[SPH_TUNE_STAGES] = {8, 8, 8, 8, 8, 8, 8, 8};
+    uint32_t tune_minb[SPH_TUNE_STAGES] = {0, 0, 0, 0, 0, 0, 0, 0};   // 1: register-capped variant
 };
 
 namespace {
@@ -154,7 +155,7 @@ uint64_t launch_key(const sph_handle *h)
     for (int st = 0; st < SPH_TUNE_STAGES; ++st) {
         const uint32_t work = st == SPH_TUNE_MERGE ? h->ncells : h->n_ub;
         k = (k ^ grid_st(h, work, st)) * 1099511628211ull;
-        k = (k ^ h->tune_bs[st]) * 1099511628211ull;
+        k = (k ^ (h->tune_bs[st] * 2u + (h->tune_minb[st] ? 1u : 0u))) * 1099511628211ull;
     }
     return k;
 }
@@ -167,10 +168,15 @@ uint64_t launch_key(const sph_handle *h)
     case 512: { constexpr int B = 512; __VA_ARGS__; } break;     \
     default: { constexpr int B = 256; __VA_ARGS__; } break;      \
     }
-#define SPH_BS_SWITCH2(bs, ...)                                  \
-    switch (bs) {                                                \
-    case 128: { constexpr int B = 128; __VA_ARGS__; } break;     \
-    default: { constexpr int B = 256; __VA_ARGS__; } break;      \
+// SWITCH2 also takes the stage's occupancy target M (minimum resident blocks
+// per SM handed to __launch_bounds__: the register cap the compiler aims for;
+// 1 = no cap).
+#define SPH_BS_SWITCH2(bs, minb, ...)                                                   \
+    switch ((bs) * 16 + ((minb) > 1 ? 1 : 0)) {                                         \
+    case 128 * 16 + 1: { constexpr int B = 128, M = 8; __VA_ARGS__; } break;            \
+    case 128 * 16: { constexpr int B = 128, M = 1; __VA_ARGS__; } break;                \
+    case 256 * 16 + 1: { constexpr int B = 256, M = 4; __VA_ARGS__; } break;            \
+    default: { constexpr int B = 256, M = 1; __VA_ARGS__; } break;                      \
     }
 
 // Exclusive scan of u32 `in` -> `out`; length from len_ptr (device) or len_const.
@@ -231,8 +237,8 @@ template <int DIM> int run_step(sph_handle *h)
     SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_DENSITY],
                   k_density<DIM, B><<<grid_st(h, nub, SPH_TUNE_DENSITY), B, 0, s>>>(c, cin, w));
     stage(h, "density");
-    SPH_BS_SWITCH2(h->tune_bs[SPH_TUNE_FORCE],
-                   k_force_integrate<DIM, B><<<grid_st(h, nub, SPH_TUNE_FORCE), B, 0, s>>>(c, cin, w));
+    SPH_BS_SWITCH2(h->tune_bs[SPH_TUNE_FORCE], h->tune_minb[SPH_TUNE_FORCE],
+                   k_force_integrate<DIM, B, M><<<grid_st(h, nub, SPH_TUNE_FORCE), B, 0, s>>>(c, cin, w));
     stage(h, "force_integrate");
     // density grid + surface mid-step: stale cell lists, integrated positions
     // (SPH-3D-2/sph_system.cpp:336-362)
@@ -244,9 +250,9 @@ template <int DIM> int run_step(sph_handle *h)
         h->grid_valid = true;
         stage(h, "surface");
     }
-    SPH_BS_SWITCH2(h->tune_bs[SPH_TUNE_ENERGY],
-                   k_energy_split<DIM, B><<<grid_st(h, nub, SPH_TUNE_ENERGY), B, 0, s>>>(c, cin, in, w,
-                                                                                       h->debug ? 1 : 0));
+    SPH_BS_SWITCH2(h->tune_bs[SPH_TUNE_ENERGY], h->tune_minb[SPH_TUNE_ENERGY],
+                   k_energy_split<DIM, B, M><<<grid_st(h, nub, SPH_TUNE_ENERGY), B, 0, s>>>(c, cin, in, w,
+                                                                                          h->debug ? 1 : 0));
     stage(h, "energy_split");
     h->last_launches += 6;
     scan_u32(h, w.split_c, w.split_rank, &cin->n, 0, &cin->n_split, 0, w.split_list);
@@ -1024,10 +1030,11 @@ int sph_surface_from_grid(sph_handle *h, const float *dens, const float *normal,
 // ---------------------------------------------------------------- launch tuning
 namespace {
 
-bool tune_valid(int st, uint32_t bs, uint32_t bpsm)
+bool tune_valid(int st, uint32_t bs, uint32_t bpsm, uint32_t cap)
 {
-    const bool big_ok = st != SPH_TUNE_FORCE && st != SPH_TUNE_ENERGY;
-    return (bs == 128 || bs == 256 || (bs == 512 && big_ok)) && bpsm >= 1 && bpsm <= 64;
+    const bool listed = st == SPH_TUNE_FORCE || st == SPH_TUNE_ENERGY;   // the two-phase list kernels
+    return (bs == 128 || bs == 256 || (bs == 512 && !listed)) && bpsm >= 1 && bpsm <= 64 && cap <= 1 &&
+           (listed || cap == 0);
 }
 
 const char *const kTuneStageName[SPH_TUNE_STAGES] = {"hash", "scatter", "reorder", "density",
@@ -1039,13 +1046,14 @@ int sph_set_tuning(sph_handle *h, const sph_tuning *t)
 {
     if (!h || !t) return SPH_ERR_INVALID;
     for (int st = 0; st < SPH_TUNE_STAGES; ++st)
-        if (!tune_valid(st, t->block[st], t->blocks_per_sm[st])) {
+        if (!tune_valid(st, t->block[st], t->blocks_per_sm[st], t->reg_cap[st])) {
             h->err = std::string("sph_set_tuning: unsupported shape for stage ") + kTuneStageName[st];
             return SPH_ERR_INVALID;
         }
     for (int st = 0; st < SPH_TUNE_STAGES; ++st) {
         h->tune_bs[st] = t->block[st];
         h->tune_bpsm[st] = t->blocks_per_sm[st];
+        h->tune_minb[st] = t->reg_cap[st];
     }
     drop_graphs(h);
     return SPH_OK;
@@ -1057,6 +1065,7 @@ int sph_get_tuning(const sph_handle *h, sph_tuning *t)
     for (int st = 0; st < SPH_TUNE_STAGES; ++st) {
         t->block[st] = h->tune_bs[st];
         t->blocks_per_sm[st] = h->tune_bpsm[st];
+        t->reg_cap[st] = h->tune_minb[st];
     }
     t->step_ms_before = t->step_ms_after = 0.0f;
     return SPH_OK;
@@ -1144,23 +1153,28 @@ int sph_autotune(sph_handle *h, uint32_t reps, sph_tuning *out)
     static const uint32_t kBpsm[5] = {2, 4, 8, 16, 32};
     for (int st = 0; st < SPH_TUNE_STAGES && !rc; ++st) {
         if (st == SPH_TUNE_MERGE && !h->cfg.use_merge) continue;
-        uint32_t best_bs = h->tune_bs[st], best_bp = h->tune_bpsm[st];
+        uint32_t best_bs = h->tune_bs[st], best_bp = h->tune_bpsm[st], best_cap = h->tune_minb[st];
         if ((rc = trial())) break;
         float best = stage_ms[st];
-        for (uint32_t bs : kBs)
-            for (uint32_t bp : kBpsm) {
-                if (!tune_valid(st, bs, bp) || (bs == best_bs && bp == best_bp)) continue;
-                h->tune_bs[st] = bs;
-                h->tune_bpsm[st] = bp;
-                if ((rc = trial())) break;
-                if (stage_ms[st] < best * 0.98f) {   // keep a change only for a clear gain
-                    best = stage_ms[st];
-                    best_bs = bs;
-                    best_bp = bp;
+        for (uint32_t cap = 0; cap <= 1 && !rc; ++cap)
+            for (uint32_t bs : kBs)
+                for (uint32_t bp : kBpsm) {
+                    if (!tune_valid(st, bs, bp, cap) || (bs == best_bs && bp == best_bp && cap == best_cap))
+                        continue;
+                    h->tune_bs[st] = bs;
+                    h->tune_bpsm[st] = bp;
+                    h->tune_minb[st] = cap;
+                    if ((rc = trial())) break;
+                    if (stage_ms[st] < best * 0.98f) {   // keep a change only for a clear gain
+                        best = stage_ms[st];
+                        best_bs = bs;
+                        best_bp = bp;
+                        best_cap = cap;
+                    }
                 }
-            }
         h->tune_bs[st] = best_bs;
         h->tune_bpsm[st] = best_bp;
+        h->tune_minb[st] = best_cap;
     }
     float after = before;
     if (!rc && !(rc = trial())) after = step_ms / reps;

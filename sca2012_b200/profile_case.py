@@ -28,6 +28,7 @@ def main():
     ap.add_argument("--adaptive", type=int, default=1)
     ap.add_argument("--block", default="")
     ap.add_argument("--bpsm", default="")
+    ap.add_argument("--regcap", default="")
     a = ap.parse_args()
     cfg = sph.preset(sph.PRESET_DAM_3D4)
     pos, vel, lvl = scenes.dam_3d4(cfg)
@@ -39,11 +40,12 @@ def main():
     cfg.use_merge = a.adaptive
     cfg.max_particle = int(len(pos) * 1.5) + 1024
     s = sph.Solver(cfg)
-    if a.block or a.bpsm:
+    if a.block or a.bpsm or a.regcap:
         t = s.get_tuning()
         block = [int(x) for x in a.block.split(",")] if a.block else t["block"]
         bpsm = [int(x) for x in a.bpsm.split(",")] if a.bpsm else t["blocks_per_sm"]
-        s.set_tuning(block, bpsm)
+        cap = [int(x) for x in a.regcap.split(",")] if a.regcap else t["reg_cap"]
+        s.set_tuning(block, bpsm, cap)
     s.set_state(dict(pos=pos, vel=vel, level=lvl))
     s.step(a.steps)
     rc = s.sync_status()
