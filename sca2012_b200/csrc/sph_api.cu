@@ -168,15 +168,16 @@ uint64_t launch_key(const sph_handle *h)
     case 512: { constexpr int B = 512; __VA_ARGS__; } break;     \
     default: { constexpr int B = 256; __VA_ARGS__; } break;      \
     }
-// SWITCH2 also takes the stage's occupancy target M (minimum resident blocks
-// per SM handed to __launch_bounds__: the register cap the compiler aims for;
-// 1 = no cap).
-#define SPH_BS_SWITCH2(bs, minb, ...)                                                   \
-    switch ((bs) * 16 + ((minb) > 1 ? 1 : 0)) {                                         \
+// SWITCH2 also sets the occupancy target M (minimum resident blocks per SM
+// handed to __launch_bounds__, i.e. the register budget the compiler works
+// to): 6 blocks of 128 / 3 of 256 (85 registers) by default, 8 / 4 (64
+// registers) for the register-capped build.
+#define SPH_BS_SWITCH2(bs, cap, ...)                                                    \
+    switch ((bs) * 16 + ((cap) ? 1 : 0)) {                                              \
     case 128 * 16 + 1: { constexpr int B = 128, M = 8; __VA_ARGS__; } break;            \
-    case 128 * 16: { constexpr int B = 128, M = 1; __VA_ARGS__; } break;                \
+    case 128 * 16: { constexpr int B = 128, M = 6; __VA_ARGS__; } break;                \
     case 256 * 16 + 1: { constexpr int B = 256, M = 4; __VA_ARGS__; } break;            \
-    default: { constexpr int B = 256, M = 1; __VA_ARGS__; } break;                      \
+    default: { constexpr int B = 256, M = 3; __VA_ARGS__; } break;                      \
     }
 
 // Exclusive scan of u32 `in` -> `out`; length from len_ptr (device) or len_const.

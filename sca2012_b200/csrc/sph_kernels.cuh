@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, const Counters *__
 // 2D SPH-2D/sph_system.cu:462-790), then the integrator and walls
 // (SPH-3D-2/sph_system.cu:204-322, SPH-2D/sph_system.cu:198-252).  The
 // integrated state goes to the *_n arrays so the loop never sees it.
-template <int DIM, int BS = kThreads, int MINB = 1>
+template <int DIM, int BS = kThreads, int MINB = 3>
 __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, const Counters *__restrict__ cnt,
                                                               WorkPtrs w)
 {
@@ -500,7 +500,7 @@ __device__ __forceinline__ float wavelet(float x, float amp)
     return amp * (x2 * 0.25f - 1.0f) * exp2f(-x2 * 0.125f * 1.44269476f);
 }
 
-template <int DIM, int BS = kThreads, int MINB = 1>
+template <int DIM, int BS = kThreads, int MINB = 3>
 __global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counters *__restrict__ cnt,
                                                            CanonPtrs st, WorkPtrs w, int want_tv)
 {
