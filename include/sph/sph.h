@@ -390,8 +390,8 @@ int sph_conserved(sph_handle *h, double out[7]);
  * thread covers).  Results do not depend on the shapes.  sph_autotune times
  * the candidates on the handle's current state (the state is restored after
  * every trial and at the end), `reps` steps per candidate, stage by stage, and
- * keeps the fastest; block in {128, 256, 512} (force and energy: 128, 256,
- * each with and without a register cap), blocks_per_sm in {2, 4, 8, 16, 32}.
+ * keeps the fastest; block in {128, 256, 512} (force and energy: 128, 256;
+ * force with and without a register cap), blocks_per_sm in {2, 4, 8, 16, 32}.
  * Defaults: 256 threads, 8 per SM, no cap.
  */
 #define SPH_TUNE_HASH     0
@@ -406,8 +406,8 @@ int sph_conserved(sph_handle *h, double out[7]);
 typedef struct sph_tuning {
     uint32_t block[SPH_TUNE_STAGES];
     uint32_t blocks_per_sm[SPH_TUNE_STAGES];   /* 1..64 */
-    uint32_t reg_cap[SPH_TUNE_STAGES];         /* force, energy: 1 = register-capped build (8 blocks of
-                                                  128 or 4 of 256 resident per SM); 0 elsewhere */
+    uint32_t reg_cap[SPH_TUNE_STAGES];         /* force: 1 = register-capped build (8 blocks of 128 or 4
+                                                  of 256 resident per SM, 64 registers); 0 elsewhere */
     float step_ms_before, step_ms_after;       /* sph_autotune: mean step time before / after */
 } sph_tuning;
 

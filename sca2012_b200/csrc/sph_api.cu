@@ -251,7 +251,7 @@ template <int DIM> int run_step(sph_handle *h)
         h->grid_valid = true;
         stage(h, "surface");
     }
-    SPH_BS_SWITCH2(h->tune_bs[SPH_TUNE_ENERGY], h->tune_minb[SPH_TUNE_ENERGY],
+    SPH_BS_SWITCH2(h->tune_bs[SPH_TUNE_ENERGY], 1,   // 64 registers fit without spills
                    k_energy_split<DIM, B, M><<<grid_st(h, nub, SPH_TUNE_ENERGY), B, 0, s>>>(c, cin, in, w,
                                                                                           h->debug ? 1 : 0));
     stage(h, "energy_split");
@@ -1035,7 +1035,7 @@ bool tune_valid(int st, uint32_t bs, uint32_t bpsm, uint32_t cap)
 {
     const bool listed = st == SPH_TUNE_FORCE || st == SPH_TUNE_ENERGY;   // the two-phase list kernels
     return (bs == 128 || bs == 256 || (bs == 512 && !listed)) && bpsm >= 1 && bpsm <= 64 && cap <= 1 &&
-           (listed || cap == 0);
+           (st == SPH_TUNE_FORCE || cap == 0);
 }
 
 const char *const kTuneStageName[SPH_TUNE_STAGES] = {"hash", "scatter", "reorder", "density",

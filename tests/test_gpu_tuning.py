@@ -48,7 +48,7 @@ def test_extreme_shapes_same_results(gpu):
     a, b = _solver(), _solver()
     n = 8
     a.set_tuning([128] * n, [2] * n)
-    b.set_tuning([512, 512, 512, 512, 256, 256, 512, 512], [32] * n, [0, 0, 0, 0, 1, 1, 0, 0])
+    b.set_tuning([512, 512, 512, 512, 256, 256, 512, 512], [32] * n, [0, 0, 0, 0, 1, 0, 0, 0])
     b.set_graph(True)
     a.step(15)
     b.step(15)
