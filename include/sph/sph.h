@@ -260,6 +260,12 @@ int sph_stage_times(sph_handle *h, float *ms, const char **names, int max, int *
  * ordering work against the step. */
 void *sph_get_stream(sph_handle *h);
 
+/* Runs the handle's work on `stream` (a cudaStream_t; NULL = the handle's own
+ * stream) from now on, after the work already queued has finished.  The caller
+ * keeps ownership of its stream and must not destroy it while the handle uses
+ * it. */
+int sph_set_stream(sph_handle *h, void *stream);
+
 /* on != 0: the step also keeps per-particle debug intermediates
  * (wavelet-transformed velocity) for sph_get_debug. */
 int sph_set_debug(sph_handle *h, int on);

@@ -13,6 +13,8 @@ import numpy as np
 
 from . import _abi
 from ._abi import Config, StateView, DebugView, MeshView  # noqa: F401
+from ._abi import (SPH_OK, SPH_ERR_INVALID, SPH_ERR_CAPACITY, SPH_ERR_CUDA, SPH_ERR_NO_DEVICE,  # noqa: F401
+                   SPH_ERR_NONFINITE, SPH_ERR_RANGE)
 from ._abi import (PRESET_REF_2D, PRESET_REF_3D2, PRESET_REF_3D4, PRESET_DAM_2D,  # noqa: F401
                    PRESET_DAM_3D2, PRESET_DAM_3D4, PRESET_ROLLOUT_3D)
 
@@ -117,6 +119,10 @@ class Solver:
             arr[s].viscosity = float(mu)
             arr[s].gas_constant = float(k)
         self._check(self._lib.sph_set_scenes(self._h, len(boxes), arr), "sph_set_scenes")
+
+    def set_stream(self, stream_ptr):
+        """Runs the handle's work on the caller's CUDA stream (0 = its own)."""
+        self._check(self._lib.sph_set_stream(self._h, C.c_void_p(int(stream_ptr) or None)), "sph_set_stream")
 
     @property
     def stream_ptr(self):

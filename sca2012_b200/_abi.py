@@ -148,6 +148,7 @@ SIGNATURES = [
     ("sph_set_profiling", C.c_int, [H, C.c_int]),
     ("sph_stage_times", C.c_int, [H, FP, C.POINTER(C.c_char_p), C.c_int, C.POINTER(C.c_int)]),
     ("sph_get_stream", C.c_void_p, [H]),
+    ("sph_set_stream", C.c_int, [H, C.c_void_p]),
     ("sph_set_debug", C.c_int, [H, C.c_int]),
     ("sph_last_launch_count", C.c_int, [H, UP]),
     ("sph_density_grid", C.c_int, [H, FP, FP]),

@@ -29,7 +29,8 @@ struct sph_handle {
     sph_config cfg;
     int device = 0;
     int num_sms = 148;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;        // where the handle's work runs
+    cudaStream_t own_stream = nullptr;    // the handle's own stream (destroyed with it)
     uint32_t cap = 0, ncells = 0;
     CanonPtrs buf[2];
     int cur = 0;
@@ -346,6 +347,7 @@ int sph_create(const sph_config *cfg, sph_handle **out)
         delete h;
         return SPH_ERR_CUDA;
     }
+    h->own_stream = h->stream;
     h->cap = cfg->max_particle;
     h->ncells = total_cells(*cfg);
     const size_t cap = h->cap, C = h->ncells;
@@ -414,7 +416,8 @@ int sph_destroy(sph_handle *h)
     for (void *p : h->allocs) cudaFree(p);
     if (h->scene_tab) cudaFree(h->scene_tab);
     if (h->cons) cudaFree(h->cons);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->stream && h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
     return SPH_OK;
 }
@@ -693,8 +696,9 @@ int sph_sync(sph_handle *h)
         cudaMemcpy(&h->cnt[h->cur], &c0, sizeof(Counters), cudaMemcpyHostToDevice);
         for (int code = 1; code < 32; ++code)
             if (err & (1u << code)) {
-                h->err = code == SPH_ERR_CAPACITY ? "particle capacity exceeded by a split (splits skipped)"
-                                                  : "device reported an error";
+                h->err = code == SPH_ERR_CAPACITY    ? "particle capacity exceeded by a split (splits skipped)"
+                         : code == SPH_ERR_NONFINITE ? "a particle's position or velocity became non-finite"
+                                                     : "device reported an error";
                 return code;
             }
     }
@@ -937,6 +941,16 @@ int sph_stage_times(sph_handle *h, float *ms, const char **names, int max, int *
 }
 
 void *sph_get_stream(sph_handle *h) { return h ? (void *)h->stream : nullptr; }
+
+int sph_set_stream(sph_handle *h, void *stream)
+{
+    if (!h) return SPH_ERR_INVALID;
+    sph_readback_wait(h);
+    cudaStreamSynchronize(h->stream);   // the handle's work so far is done before the switch
+    drop_graphs(h);                     // recaptured on the next graph step
+    h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+    return cuda_check(h, "sph_set_stream");
+}
 
 int sph_last_launch_count(const sph_handle *h, uint32_t *launches)
 {

@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, const Counters *__
 // (SPH-3D-2/sph_system.cu:204-322, SPH-2D/sph_system.cu:198-252).  The
 // integrated state goes to the *_n arrays so the loop never sees it.
 template <int DIM, int BS = kThreads, int MINB = 3>
-__global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, const Counters *__restrict__ cnt,
+__global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Counters *__restrict__ cnt,
                                                               WorkPtrs w)
 {
     __shared__ uint32_t nlist[kListLen][BS];
@@ -478,6 +478,10 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, cons
             if (DIM == 3) wall(x.z, v.z, lo.z, blo.z, bhi.z, 2);
             if (w.wall) w.wall[s] = hit;   // recorded for the adjoint
         }
+        // a non-finite position is reported (the walls would hide +-inf); the
+        // neighbour tests fail for it, so it interacts with nothing
+        if (!(isfinite(x.x) && isfinite(x.y) && isfinite(x.z)) || !isfinite(v.x + v.y + v.z))
+            atomicOr(&cnt->error, 1u << SPH_ERR_NONFINITE);
         if (c.integrator != SPH_INTEGRATE_REF2D) {
             ev.x = (ev.x + v.x) / 2.0f; ev.y = (ev.y + v.y) / 2.0f; ev.z = (ev.z + v.z) / 2.0f;
         }

@@ -16,12 +16,25 @@ from tests._parity import check_close, check_equal
 
 pytestmark = pytest.mark.gpu
 
+def _obstacles(c):
+    c.use_cylinder = 1       # the reference's three spheres (SPH-3D-2/sph_system.cu:242-282)
+    c.push_left = 1          # push force (SPH-3D-2/sph_system.cu:229-236)
+
+
+def _mouse(c):
+    c.extern_force_on = 1    # 2D mouse force (SPH-2D/sph_system.cu:781-789)
+    c.extern_click[0], c.extern_click[1] = 8.0, 8.0
+    c.extern_force[0], c.extern_force[1] = 3.0, -2.0
+
+
 CASES = {
     "ref_2d": (sph.PRESET_REF_2D, scenes.ref_init_2d, 10),
     "ref_3d2": (sph.PRESET_REF_3D2, scenes.ref_box_3d2, 8),
     "ref_3d4": (sph.PRESET_REF_3D4, lambda c: _crop(scenes.ref_box_3d4(c), 14.0), 4),
     "dam_2d": (sph.PRESET_DAM_2D, scenes.dam_2d, 3),
     "dam_3d2_small": (sph.PRESET_DAM_3D2, lambda c: scenes.block_3d(c, (24, 24, 12), 0.01, seed=3), 3),
+    "ref_3d2_obstacles": (sph.PRESET_REF_3D2, scenes.ref_box_3d2, 8, _obstacles),
+    "ref_2d_mouse": (sph.PRESET_REF_2D, scenes.ref_init_2d, 10, _mouse),
 }
 
 
@@ -31,19 +44,22 @@ def _crop(scene, xmax):
     return pos[m], vel[m], lvl[m]
 
 
-def _cfg(preset, split, merge, n):
+def _cfg(preset, split, merge, n, extra=None):
     c = sph.preset(preset)
     c.use_split = int(split)
     c.use_merge = int(merge)
     c.max_particle = max(4 * n * (c.split_ways - 1) + n, 1024)
+    if extra:
+        extra(c)
     return c
 
 
 def run_case(name):
-    preset, scene, warm = CASES[name]
+    preset, scene, warm, *more = CASES[name]
+    extra = more[0] if more else None
     pos, vel, lvl = scene(sph.preset(preset))
-    cfg_on = _cfg(preset, 1, 1, len(pos))
-    cfg_off = _cfg(preset, 0, 0, len(pos))
+    cfg_on = _cfg(preset, 1, 1, len(pos), extra)
+    cfg_off = _cfg(preset, 0, 0, len(pos), extra)
     s = sph.Solver(cfg_on)
     s.set_debug(True)
     s.set_state(dict(pos=pos, vel=vel, level=lvl))
