@@ -69,6 +69,7 @@ def parse():
     p.add_argument("--batch-scenes", type=int, default=256, help="0 skips the batched-scenes comparison")
     p.add_argument("--batch-steps", type=int, default=20)
     p.add_argument("--rollout-steps", type=int, default=200, help="0 skips the differentiable-rollout timing")
+    p.add_argument("--other-configs", type=int, default=1, help="0 skips the smaller workloads and CPU detail")
     return p.parse_args()
 
 
@@ -249,6 +250,10 @@ def run_ours(args, rank, world, local_rank):
     achieved = alg / (stage_avg[top] * 1e-3) / 1e9
     traffic_full, n_full = profiled_traffic(top)
     traffic = traffic_full * (n_avg / n_full) if traffic_full and n_full else None
+    # the three neighbour loops together against their compulsory bytes
+    # (density 28 + force 64 + energy 36 = 128 B per particle-step)
+    nl_ms = sum(stage_avg.get(k, 0.0) for k in ("density", "force_integrate", "energy_split"))
+    nl_gbs = 128.0 * n_avg / (nl_ms * 1e-3) / 1e9 if nl_ms else None
 
     # --- plain (non-adaptive) step on the same state, for the "vs plain" ratio
     plain = cfg.copy()
@@ -319,7 +324,8 @@ def run_ours(args, rank, world, local_rank):
         rs.close()
     small["particles_initial"] = len(rpos)
 
-    batched = batched_scenes(args) if (world == 1 and args.batch_scenes) else None
+    batched = batched_scenes(args, rank, world) if args.batch_scenes else None
+    others = small_configs(args) if (world == 1 and not args.no_cpu_baseline and args.other_configs) else None
     roll = rollout_bench(args) if (world == 1 and args.rollout_steps) else None
 
     out = None
@@ -347,12 +353,16 @@ def run_ours(args, rank, world, local_rank):
                          "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_particle": STAGE_BYTES.get(top),
                          "launch_ms": stage_avg[top], "peak_source": peak_src,
-                         "note": "neighbour loops are FP32-issue bound: the HBM fraction is low by design"},
+                         "note": "neighbour loops are FP32-issue bound: the HBM fraction is low by design",
+                         "neighbour_loops": {"stages": ["density", "force_integrate", "energy_split"],
+                                             "bytes_per_particle": 128, "ms": nl_ms, "achieved": nl_gbs,
+                                             "frac": nl_gbs / peak if nl_gbs else None}},
             "stages_ms": stage_avg,
             "tuning": tuning,
             "conserved": conserved,
             "ref_3d2_default_scene": small,
             "batched_scenes": batched,
+            "other_configs": others,
             "rollout": roll,
             "cpu_baseline": cpu,
             "clocks": clk,
@@ -362,8 +372,52 @@ def run_ours(args, rank, world, local_rank):
     return out
 
 
+# ----------------------------------------------------------------- other configurations
+def small_configs(args):
+    """The 2D plain dam break (4,096 particles, no adaptivity, 1,000-step
+    config) and the 3D two-way dam break (131,072 particles, 500-step config)
+    on the GPU, eager and CUDA-graph, 200 timed steps each; and the FP64
+    oracle on the host, one thread and all threads, a few steps of each of
+    the three workloads (particle-steps/s)."""
+    import torch
+    import sca2012_b200 as sph
+    from sca2012_b200 import scenes as sc
+    from oracle import oracle as O
+    cases = {"dam_2d_4096": (sph.PRESET_DAM_2D, sc.dam_2d, 0), "dam_3d2_131072": (sph.PRESET_DAM_3D2, sc.dam_3d2, 1)}
+    gpu, cpu = {}, {}
+    for name, (pre, make, adapt) in cases.items():
+        cfg = sph.preset(pre)
+        cfg.use_split = cfg.use_merge = adapt
+        pos, vel, lvl = make(cfg, seed=args.seed)
+        for mode in ("eager", "graph"):
+            s = sph.Solver(cfg)
+            s.set_graph(mode == "graph")
+            s.set_state(dict(pos=pos, vel=vel, level=lvl))
+            s.step(5)
+            st = torch.cuda.ExternalStream(s.stream_ptr)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            n_before = s.num_particles()
+            a.record(st)
+            s.step(200)
+            b.record(st)
+            b.synchronize()
+            n_after = s.num_particles()
+            gpu.setdefault(name, {})[mode] = 200 * 0.5 * (n_before + n_after) / (a.elapsed_time(b) * 1e-3)
+            s.close()
+        for th in (1, os.cpu_count() or 1):
+            v, used, _ = cpu_baseline(cfg, pos, vel, lvl, 3 if adapt else 10, threads=th)
+            cpu.setdefault(name, {})[f"threads_{used}"] = v
+    cfg, pos, vel, lvl = load_workload(args.seed)
+    for th in (1, os.cpu_count() or 1):
+        v, used, _ = cpu_baseline(cfg, pos, vel, lvl, 1, threads=th)
+        cpu.setdefault("dam_3d4_1114112", {})[f"threads_{used}"] = v
+    O.set_threads(0)
+    return {"gpu_particle_steps_per_s": gpu, "cpu_oracle_particle_steps_per_s": cpu,
+            "cpu_cores": os.cpu_count(), "note": "GPU: CUDA events, count averaged over the window"}
+
+
 # ----------------------------------------------------------------- batched scenes
-def batched_scenes(args):
+def batched_scenes(args, rank=0, world=1):
     """256 independent dam-break scenes (128 2D, 128 3D two-way; sizes
     log-uniform in [1024, 65536], per-scene viscosity and stiffness), split
     and merge on.  Batched: one handle per dimensionality holding all its
@@ -371,7 +425,10 @@ def batched_scenes(args):
     scene in its own box-sized world with plain (eager) launches, stepped
     (a) one scene at a time, each synchronised before the next, and (b) all
     handles' streams at once.  Scene-steps/s by wall clock around
-    synchronised loops (the baselines span 256 streams)."""
+    synchronised loops (the baselines span 256 streams).  With N > 1 ranks
+    the scenes are sharded (scene k on rank k mod N, no collective in the
+    step) and only the batched figure is taken: all scenes / the slowest
+    rank's time."""
     import torch
     import sca2012_b200 as sph
     from sca2012_b200 import scenes as sc
@@ -381,7 +438,8 @@ def batched_scenes(args):
     for pre, seed in ((sph.PRESET_DAM_2D, args.seed + 11), (sph.PRESET_DAM_3D2, args.seed + 12)):
         base = sph.preset(pre)
         base.use_split = base.use_merge = 1
-        batches.append(sc.batch_scenes(base, half, seed=seed))
+        mine = [k for k in range(half) if k % world == rank]
+        batches.append(sc.batch_scenes(base, half, seed=seed, subset=mine if world > 1 else None))
 
     def timed_call(fn):
         torch.cuda.synchronize()
@@ -414,6 +472,15 @@ def batched_scenes(args):
     timed(bs, 3)
     t_batched = timed(bs, steps)
     status = 0
+    if world > 1:
+        n_mine = sum(len(b[1]) for b in batches)
+        t_all, n_all = reduce_over_ranks(t_batched, float(n_mine), True, "cuda")
+        for h in bs:
+            status |= h.sync_status()
+            h.close()
+        return {"scenes": int(n_all), "ranks": world, "steps": steps, "sharding": "scene k on rank k mod N",
+                "batched_scene_steps_per_s": n_all * steps / t_all, "status": status,
+                "timing": "wall clock around synchronised step loops, slowest rank"}
     # the adjoint of the last 50 steps, batched: checkpointed forward, a
     # density-grid loss over every scene (nodes at cell centres), backward
     t_fwd = t_bwd = 0.0

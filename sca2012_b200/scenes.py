@@ -191,7 +191,7 @@ def block_3d(cfg, counts=(32, 32, 32), spacing=0.01, seed=0):
     return pos, np.zeros_like(pos), np.ones(len(pos), np.uint32)
 
 
-def batch_scenes(cfg, count, seed=0, n_min=1024, n_max=65536, gap_cells=2):
+def batch_scenes(cfg, count, seed=0, n_min=1024, n_max=65536, gap_cells=2, subset=None):
     """`count` independent dam-break scenes packed into one world for a
     batched handle (sph_set_scenes).
 
@@ -205,10 +205,13 @@ def batch_scenes(cfg, count, seed=0, n_min=1024, n_max=65536, gap_cells=2):
     cells.  Boxes sit at whole-cell offsets, `gap_cells` apart, packed in
     shelves over the x-z plane (3D) or the x-y plane (2D).
 
+    `subset` (a list of scene numbers) packs only those scenes, each drawn
+    exactly as in the full set (e.g. one rank's share of a sharded batch).
+
     Returns (cfg, boxes, pos, vel, level, scene, counts): cfg is a copy with
     world, ncell and max_particle (4x the particles) set; boxes is a list of
     (lo, hi, viscosity, gas_constant) for Solver.set_scenes; particles are
-    scene by scene in scene order."""
+    scene by scene in scene order (scene index = position in the subset)."""
     dim = int(cfg.dim)
     s = float(cfg.kernel[0]) * 0.5
     cs = float(cfg.cell_size)
@@ -220,6 +223,11 @@ def batch_scenes(cfg, count, seed=0, n_min=1024, n_max=65536, gap_cells=2):
     mu = np.exp(np.log(1e-3) + uniform(seed, k, 21) * (np.log(1e-1) - np.log(1e-3)))
     stiff = 1.0 + 4.0 * uniform(seed, k, 22)
     blocks = np.maximum(4, np.rint(n_target[:, None] ** (1.0 / dim) * asp)).astype(np.int64)
+    first_of = np.concatenate([[0], np.cumsum(np.prod(blocks, axis=1))])   # jitter ids as in the full set
+    if subset is not None:
+        subset = np.asarray(subset, np.int64)
+        blocks, mu, stiff, first_of = blocks[subset], mu[subset], stiff[subset], first_of[subset]
+        count = len(subset)
     # box extents in cells
     ext = np.zeros((count, dim), np.int64)
     ext[:, 0] = np.ceil(2.0 * blocks[:, 0] * s / cs - 1e-9)
@@ -251,13 +259,12 @@ def batch_scenes(cfg, count, seed=0, n_min=1024, n_max=65536, gap_cells=2):
         out.ncell[2] = 1
         out.world[2] = 0.0
     boxes, parts, scene = [], [], []
-    first = 0
     for i in range(count):
         lo = [f32(off[i, a]) * f32(cs) for a in range(dim)]
         hi = [f32(top[i, a]) * f32(cs) for a in range(dim)]
         boxes.append((lo, hi, float(f32(mu[i])), float(f32(stiff[i]))))
-        p = lattice(tuple(int(b) for b in blocks[i]), s, np.array(lo, np.float64), seed, first_index=first)
-        first += len(p)
+        p = lattice(tuple(int(b) for b in blocks[i]), s, np.array(lo, np.float64), seed,
+                    first_index=int(first_of[i]))
         parts.append(p)
         scene.append(np.full(len(p), i, np.uint32))
     pos = np.concatenate(parts)
