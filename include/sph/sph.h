@@ -143,6 +143,9 @@ typedef struct sph_config {
     uint32_t max_triangles;  /* device mesh capacity (0: 3 per grid node) */
     uint32_t compensated_positions; /* 1: positions carry an FP32 low part and x += v dt is a
                                        compensated (Fast2Sum) update; 0: plain FP32 (reference) */
+    float close_r2;          /* the force loop (and the energy loop with energy_skip_close) skips
+                                pairs with r^2 below this: reference 1e-4, a constant of its unit
+                                system (SPH-3D-2/sph_system.cu:801-804, SPH-2D/sph_system.cu:584) */
 } sph_config;
 
 /* Host view of a particle state (SoA).  Vectors hold `dim` floats per

@@ -229,7 +229,7 @@ void oracle_force(const sph_config *c, uint32_t n, const float *pos, const float
                 float r2f = r2_f32(c, pi, pj);
                 float maxh2 = c->kernel2[li] > c->kernel2[lj] ? c->kernel2[li] : c->kernel2[lj];
                 if (!(r2f < maxh2)) continue;             /* :797-799 */
-                if (r2f < 0.0001f) continue;              /* :801-804 */
+                if (r2f < c->close_r2) continue;          /* :801-804 (1e-4 in the reference) */
                 float rf = sqrtf(r2f);
                 double rel[3] = {0, 0, 0}, r2 = 0.0;
                 for (int a = 0; a < d; ++a) {
@@ -428,7 +428,7 @@ void oracle_energy(const sph_config *c, uint32_t n, const float *pos, const floa
                 const float *pj = pos + (size_t)j * d;
                 float r2f = r2_f32(c, pi, pj);
                 if (!(r2f < h2)) continue;                        /* :1227 */
-                if (c->energy_skip_close && r2f < 0.0001f) continue;  /* :1229-1232 */
+                if (c->energy_skip_close && r2f < c->close_r2) continue;  /* :1229-1232 */
                 for (int a = 0; a < d; ++a) {
                     double t = wavelet(((double)pi[a] - (double)pj[a]) / h);   /* :1238-1240 */
                     tsum[a] += t;

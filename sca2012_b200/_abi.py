@@ -63,7 +63,7 @@ class Config(C.Structure):
         ("extern_len", C.c_float), ("extern_coe", C.c_float),
         ("dens_mul", C.c_uint32), ("den_size", C.c_float), ("ndens", U3), ("iso_value", C.c_float),
         ("mc_interpolate", C.c_uint32), ("splat_with_kernel", C.c_uint32), ("grid_every", C.c_uint32),
-        ("max_triangles", C.c_uint32), ("compensated_positions", C.c_uint32),
+        ("max_triangles", C.c_uint32), ("compensated_positions", C.c_uint32), ("close_r2", C.c_float),
     ]
 
     def copy(self):

@@ -21,7 +21,7 @@
 //   adj_density    rho_i = sum_j m_j W_i(r_ij): each slot gathers the terms
 //                  of its own density and of its neighbours' densities
 // Neighbour pairs are re-derived from the taped FP32 positions with the
-// forward's own predicates (r^2 < max(h_i^2, h_j^2), r^2 >= 1e-4 for forces;
+// forward's own predicates (r^2 < max(h_i^2, h_j^2), r^2 >= close_r2 for forces;
 // r^2 < h_i^2 for densities; h - r > 0 for each kernel's term), so the pair
 // sets are exactly the forward's.
 #pragma once
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kThreads) adj_force(sph_config c, StepCounts k
                     float rx, ry, rz;
                     const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
                     const float cut = pj.w == 1.0f ? cut0 : cut1;
-                    if (!(r2 < cut) || r2 < 0.0001f) continue;
+                    if (!(r2 < cut) || r2 < c.close_r2) continue;
                     const int lj = lv(pj.w);
                     const float r = __fsqrt_rn(r2);
                     const float ikr = __fsub_rn(hi, r), jkr = __fsub_rn(c.kernel[lj], r);
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(kThreads) k_topo_pairs(sph_config c, StepCount
                     }
                     const float r2 = r2_of<DIM>(pi, pj, dx, dy_, dz_);
                     const float cut = pj.w == 1.0f ? cut0 : cut1;
-                    if (r2 < cut && !(r2 < 0.0001f)) {
+                    if (r2 < cut && !(r2 < c.close_r2)) {
                         if (FILL) {
                             const float r = __fsqrt_rn(r2);
                             const uint32_t fi = __fsub_rn(hi, r) > 0.0f ? 1u << 30 : 0u;

@@ -124,6 +124,7 @@ void preset_ref_3d(sph_config *c, bool four_way)
     c->surface_threshold = 0.8f;
     c->co_energy = 1.0f;
     c->density_skip_r2 = 0.0001f;
+    c->close_r2 = 0.0001f;          // sph_system.cu:801-804, :1229-1232
     c->lapc_three_quarters = 0.0f;  // integer 3/4 (sph_system.cu:828)
     c->integrator = SPH_INTEGRATE_REF3D;
     c->kernel_h6_twice = 1;
@@ -159,6 +160,7 @@ void preset_ref_2d(sph_config *c)
     c->split_criteria = 0.7f;       // m_thresh_split
     c->merge_criteria = 0.04f;      // m_thresh_merge
     c->density_skip_r2 = 1e-12f;    // EXT2 (SPH-2D/sph_system.cu:8,396)
+    c->close_r2 = 0.0001f;          // force loop (SPH-2D/sph_system.cu:584)
     c->lapc_three_quarters = 0.0f;
     c->split_ways = 2;
     c->integrator = SPH_INTEGRATE_REF2D;
@@ -225,6 +227,10 @@ void preset_si(sph_config *c, int dim, float s, uint32_t ways, float dt)
     c->co_surface = 0.0f;
     c->co_energy = 0.0f;
     c->density_skip_r2 = 0.0f;
+    // the reference's 1e-4 is a length of its own units (h ~ 1); at h = 2s
+    // in metres it would drop every pair inside 0.01 m.  Only (nearly)
+    // coincident pairs are skipped here.
+    c->close_r2 = (1e-3f * h) * (1e-3f * h);
     c->lapc_three_quarters = 0.75f;
     c->split_ways = ways;
     c->integrator = SPH_INTEGRATE_PHYS;

@@ -319,8 +319,9 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
         float fx = 0.f, fy = 0.f, fz = 0.f, gx = 0.f, gy = 0.f, gz = 0.f, lap = 0.f;
         if (DIM == 2)   // self term, SPH-2D/sph_system.cu:599-603 (0 with the integer 3/4)
             lap += ilap * ai.w * hi2 * (0.0f - c.lapc_three_quarters * hi2);
-        // pairs with r^2 < max(h_i^2, h_j^2) and r^2 >= 1e-4 (:797-804)
+        // pairs with r^2 < max(h_i^2, h_j^2) and r^2 >= close_r2 (:797-804)
         const float cut0 = fmaxf(hi2, c.kernel2[0]), cut1 = fmaxf(hi2, c.kernel2[1]);
+        const float close = c.close_r2;
         uint32_t *my_list = &nlist[0][threadIdx.x];
         uint32_t cntl = 0;
         // phase B: the interaction math over the listed neighbours
@@ -365,7 +366,7 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
             float rx, ry, rz;
             const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
             const float cut = pj.w == 1.0f ? cut0 : cut1;
-            if (t != s && r2 < cut && !(r2 < 0.0001f)) {
+            if (t != s && r2 < cut && !(r2 < close)) {
                 my_list[cntl * BS] = t;
                 if (++cntl == kListLen) flush();
             }
@@ -520,7 +521,7 @@ __global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counter
         const float ih = 1.0f / h, isq = 1.0f / sqrtf(h);
         const uint3 q = cell_of<DIM>(c, pi);
         float tsx = 0.f, tsy = 0.f, tsz = 0.f, tvx = 0.f, tvy = 0.f, tvz = 0.f;
-        const float skip = c.energy_skip_close ? 0.0001f : 0.0f;   // :1229-1232 (2D keeps close pairs)
+        const float skip = c.energy_skip_close ? c.close_r2 : 0.0f;   // :1229-1232 (2D keeps close pairs)
         uint32_t *my_list = &nlist[0][threadIdx.x];
         uint32_t cntl = 0;
         // phase B: the wavelet transform over the listed neighbours

@@ -22,7 +22,7 @@ def _pairs(cfg, x, level):
             if j != i and r2[j] < h[i] ** 2:
                 d_nbr.append(j)
         for j in range(n):
-            if j != i and r2[j] < max(h[i], h[j]) ** 2 and r2[j] >= 1e-4:
+            if j != i and r2[j] < max(h[i], h[j]) ** 2 and r2[j] >= cfg.close_r2:
                 r = np.sqrt(r2[j])
                 f_nbr.append(j | (int(h[i] - r > 0) << 30) | (int(h[j] - r > 0) << 31))
         d_off.append(len(d_nbr))
