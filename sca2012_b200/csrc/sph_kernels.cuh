@@ -222,37 +222,31 @@ __global__ void __launch_bounds__(BS) k_reorder(const Counters *__restrict__ cnt
     }
 }
 
-// ------------------------------------------------------------ warp-cooperative pair loop
+// ------------------------------------------------------------ warp-lockstep pair loop
 // The force and energy loops walk each particle's 3^DIM-cell stencil with the
-// particle's whole warp in lockstep (up to 4 candidates per lane per step).
-// A lane appends the candidates it accepts to its short list in shared
-// memory; as soon as any lane's list holds kWarpCap entries, the warp
-// processes every listed pair together: pair p of the warp (lanes' lists
-// concatenated) is computed by lane p mod 32, its NT terms go through shared
-// memory, and each owner adds its own pairs' terms in list order.  So the
-// expensive pair math runs on all 32 lanes however unevenly the neighbours
-// fall, and every particle's sums take the same order whichever particles
-// share its warp (results do not depend on the launch shape or on the
-// scenes batched beside it).
-constexpr uint32_t kWarpCap = 8;              // list fill that triggers a warp flush
+// particle's whole warp in lockstep (up to 4 candidates per lane per step,
+// their loads in flight together).  A lane appends the candidates it accepts
+// to its list in shared memory; as soon as any lane's list holds kWarpCap
+// entries, the whole warp runs the pair math over the lists in rounds (round
+// k: every lane's k-th entry), each lane adding into its own sums in list
+// order.  Flushing together keeps the expensive pair math converged (lists
+// fill at similar rates, so few lanes idle in a round), and every particle's
+// sums take the same order whichever particles share its warp.
+constexpr uint32_t kWarpCap = 24;             // list fill that triggers a warp flush
 constexpr uint32_t kWarpSlot = kWarpCap + 4;  // a step can add 4 more before the check
 
-template <int NT>
 struct WarpPairSmem {
     uint32_t lst[kWarpSlot][32];     // per-lane lists, entry-major (appends hit 32 banks)
-    uint32_t excl[32];               // each lane's first position in the warp's concatenation
-    uint8_t omap[32 * kWarpSlot];    // position -> owner lane
-    float res[NT][32];               // one round's pair terms
 };
 
 // accept(t, pj): this lane's test of candidate slot t at position pj.
-// pair(o, t, term): the NT terms of (owner lane o, neighbour slot t).
-// acc: this lane's sums.  Every lane of the warp must call it (active =
-// false for a lane without a particle).
-template <int DIM, int NT, class Accept, class Pair>
+// pair(t): adds this lane's pair with neighbour slot t into its sums.
+// Every lane of the warp must call it (active = false for a lane without a
+// particle).
+template <int DIM, class Accept, class Pair>
 __device__ __forceinline__ void warp_pairs(const sph_config &c, const uint32_t *__restrict__ off,
                                            const float4 *__restrict__ pos, bool active, uint3 q,
-                                           WarpPairSmem<NT> &sm, float (&acc)[NT], Accept accept, Pair pair)
+                                           WarpPairSmem &sm, Accept accept, Pair pair)
 {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -273,37 +267,11 @@ __device__ __forceinline__ void warp_pairs(const sph_config &c, const uint32_t *
     };
     uint32_t cnt = 0;
     auto flush = [&]() {
-        uint32_t inc = cnt;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t y = __shfl_up_sync(full, inc, d);
-            if (lane >= d) inc += y;
-        }
-        const uint32_t excl = inc - cnt;
-        const uint32_t total = __shfl_sync(full, inc, 31);
-        sm.excl[lane] = excl;
-        for (uint32_t k = 0; k < cnt; ++k) sm.omap[excl + k] = (uint8_t)lane;
-        __syncwarp();
-        for (uint32_t r0 = 0; r0 < total; r0 += 32) {
-            const uint32_t p = r0 + lane;
-            float term[NT];
-#pragma unroll
-            for (int k = 0; k < NT; ++k) term[k] = 0.0f;
-            if (p < total) {
-                const int o = sm.omap[p];
-                pair(o, sm.lst[p - sm.excl[o]][o], term);
-            }
-#pragma unroll
-            for (int k = 0; k < NT; ++k) sm.res[k][lane] = term[k];
-            __syncwarp();
-            const uint32_t lo = max(excl, r0), hi = min(excl + cnt, r0 + 32u);
-            for (uint32_t qq = lo; qq < hi; ++qq) {
-#pragma unroll
-                for (int k = 0; k < NT; ++k) acc[k] += sm.res[k][qq - r0];
-            }
-            __syncwarp();
-        }
+        const uint32_t m = __reduce_max_sync(full, cnt);
+        for (uint32_t k = 0; k < m; ++k)
+            if (k < cnt) pair(sm.lst[k][lane]);
         cnt = 0;
+        __syncwarp();
     };
     bool more = active && next_row();
     while (__any_sync(full, more)) {
@@ -388,8 +356,7 @@ template <int DIM, int BS = kThreads, int MINB = 3>
 __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Counters *__restrict__ cnt,
                                                               WorkPtrs w)
 {
-    __shared__ WarpPairSmem<7> smem[BS / 32];
-    __shared__ float4 own_pos[BS / 32][32], own_ev[BS / 32][32], own_aux[BS / 32][32];
+    __shared__ WarpPairSmem smem[BS / 32];
     const uint32_t n = cnt->n;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     // warp-uniform grid-stride loop: a warp takes 32 consecutive slots
@@ -401,8 +368,11 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
         const float4 evi = w.sev[s];
         const float4 ai = w.saux[s];   // rho, p, p/rho^2, m/rho
         const int li = lv(pi.w);
-        const float hi2 = c.kernel2[li];
+        const float hi = c.kernel[li], hi2 = c.kernel2[li];
         const float mi = c.mass[li];
+        const float ispk = c.kernel_h6_twice ? c.spiky[li] / c.kernel6[li] : c.spiky[li];
+        const float ivis = c.kernel_h6_twice ? c.visco[li] / c.kernel6[li] : c.visco[li];
+        const float igrad = -c.grad_poly6[li];
         const float ilap = c.lapc_poly6[li];
         const uint32_t sid = w.nscenes ? min(w.sscene[s], w.nscenes - 1u) : 0u;
         const float visc = w.nscenes ? w.scene_tab[2 * sid].w : c.viscosity;
@@ -411,10 +381,9 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
         q.x = k % c.ncell[0];
         q.y = (k / c.ncell[0]) % c.ncell[1];
         q.z = DIM == 3 ? k / (c.ncell[0] * c.ncell[1]) : 0u;
-        own_pos[wib][lane] = pi;
-        own_ev[wib][lane] = make_float4(evi.x, evi.y, evi.z, visc);
-        own_aux[wib][lane] = ai;
-        __syncwarp();
+        float fx = 0.f, fy = 0.f, fz = 0.f, gx = 0.f, gy = 0.f, gz = 0.f, lap = 0.f;
+        if (DIM == 2)   // self term, SPH-2D/sph_system.cu:599-603 (0 with the integer 3/4)
+            lap += ilap * ai.w * hi2 * (0.0f - c.lapc_three_quarters * hi2);
         // pairs with r^2 < max(h_i^2, h_j^2) and r^2 >= close_r2 (:797-804)
         const float cut0 = fmaxf(hi2, c.kernel2[0]), cut1 = fmaxf(hi2, c.kernel2[1]);
         const float close = c.close_r2;
@@ -424,30 +393,24 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
             const float cut = pj.w == 1.0f ? cut0 : cut1;
             return t != s && r2 < cut && !(r2 < close);
         };
-        // the pair terms of owner lane o and neighbour slot t:
-        // force (3), colour-field gradient (3), colour-field Laplacian (1)
-        auto pair = [&](int o, uint32_t t, float (&term)[7]) {
-            const float4 po = own_pos[wib][o], eo = own_ev[wib][o], ao = own_aux[wib][o];
-            const int lo_ = lv(po.w);
-            const float ho = c.kernel[lo_], ho2 = c.kernel2[lo_], mo = c.mass[lo_];
-            const float ospk = c.kernel_h6_twice ? c.spiky[lo_] / c.kernel6[lo_] : c.spiky[lo_];
-            const float ovis = c.kernel_h6_twice ? c.visco[lo_] / c.kernel6[lo_] : c.visco[lo_];
+        // pressure, viscosity and colour-field terms of one neighbour
+        auto pair = [&](uint32_t t) {
             const float4 pj = w.spos[t];
             const float4 aj = w.saux[t];
             const float4 evj = w.sev[t];
             float rx, ry, rz;
-            const float r2 = r2_of<DIM>(po, pj, rx, ry, rz);
+            const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
             const int lj = lv(pj.w);
             const float r = __fsqrt_rn(r2);
             float ipk = 0.f, ivk = 0.f, jpk = 0.f, jvk = 0.f;
-            const float ikr = __fsub_rn(ho, r);
+            const float ikr = __fsub_rn(hi, r);
             if (ikr > 0.0f) {
-                ipk = ospk * ikr * ikr;
-                ivk = ovis * ikr;
-                const float x = ho2 - r2;
-                const float tg = -c.grad_poly6[lo_] * aj.w * x * x;   // -grad_poly6 * m_j/rho_j * (h^2-r^2)^2
-                term[3] = tg * rx; term[4] = tg * ry; term[5] = tg * rz;
-                term[6] = c.lapc_poly6[lo_] * aj.w * x * (r2 - c.lapc_three_quarters * x);
+                ipk = ispk * ikr * ikr;
+                ivk = ivis * ikr;
+                const float x = hi2 - r2;
+                const float tg = igrad * aj.w * x * x;   // -grad_poly6 * m_j/rho_j * (h^2-r^2)^2
+                gx += tg * rx; gy += tg * ry; gz += tg * rz;
+                lap += ilap * aj.w * x * (r2 - c.lapc_three_quarters * x);
             }
             const float jkr = __fsub_rn(c.kernel[lj], r);
             if (jkr > 0.0f) {
@@ -457,19 +420,14 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
                 jvk = jvis * jkr;
             }
             const float mj = c.mass[lj];
-            const float tp = mo * mj * (ao.z + aj.z) * (ipk + jpk) * 0.5f / r;
-            const float tv = (ao.w * aj.w) * eo.w * (ivk + jvk) * 0.5f;
-            term[0] = -rx * tp + (evj.x - eo.x) * tv;
-            term[1] = -ry * tp + (evj.y - eo.y) * tv;
-            term[2] = DIM == 3 ? -rz * tp + (evj.z - eo.z) * tv : 0.0f;
+            const float tp = mi * mj * (ai.z + aj.z) * (ipk + jpk) * 0.5f / r;
+            const float tv = (ai.w * aj.w) * visc * (ivk + jvk) * 0.5f;
+            fx += -rx * tp + (evj.x - evi.x) * tv;
+            fy += -ry * tp + (evj.y - evi.y) * tv;
+            if (DIM == 3) fz += -rz * tp + (evj.z - evi.z) * tv;
         };
-        float acc[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (DIM == 2)   // self term, SPH-2D/sph_system.cu:599-603 (0 with the integer 3/4)
-            acc[6] = ilap * ai.w * hi2 * (0.0f - c.lapc_three_quarters * hi2);
-        warp_pairs<DIM, 7>(c, w.cell_off, w.spos, valid, q, smem[wib], acc, accept, pair);
+        warp_pairs<DIM>(c, w.cell_off, w.spos, valid, q, smem[wib], accept, pair);
         if (!valid) continue;
-        float fx = acc[0], fy = acc[1], fz = acc[2];
-        const float gx = acc[3], gy = acc[4], gz = acc[5], lap = acc[6];
         // surface tension switch (SPH-3D-2/sph_system.cu:1113-1136)
         const float nrm = sqrtf(gx * gx + gy * gy + gz * gz);
         if (nrm > c.surface_threshold) {
@@ -591,8 +549,7 @@ template <int DIM, int BS = kThreads, int MINB = 3>
 __global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counters *__restrict__ cnt,
                                                            CanonPtrs st, WorkPtrs w, int want_tv)
 {
-    __shared__ WarpPairSmem<6> smem[BS / 32];
-    __shared__ float4 own_pos[BS / 32][32];
+    __shared__ WarpPairSmem smem[BS / 32];
     const uint32_t n = cnt->n;
     // 2/(PI^0.25 * sqrt(3 sigma)) with PI = 3.141592f, sigma = 2
     const float amp = 2.0f / (powf(3.141592f, 0.25f) * sqrtf(6.0f));
@@ -604,40 +561,34 @@ __global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counter
         const float4 pi = w.spos_n[s];
         const int li = lv(pi.w);
         const int lk = c.energy_large_kernel ? 0 : li;
-        const float h2 = c.kernel2[lk];
+        const float h = c.kernel[lk], h2 = c.kernel2[lk];
+        const float ih = 1.0f / h, isq = 1.0f / sqrtf(h);
         const uint3 q = cell_of<DIM>(c, pi);
+        float tsx = 0.f, tsy = 0.f, tsz = 0.f, tvx = 0.f, tvy = 0.f, tvz = 0.f;
         const float skip = c.energy_skip_close ? c.close_r2 : 0.0f;   // :1229-1232 (2D keeps close pairs)
-        own_pos[wib][lane] = pi;
-        __syncwarp();
         // j != i with skip <= r^2 < h^2 (:1222-1233), on the stale lists
         auto accept = [&](uint32_t t, const float4 &pj) {
             float rx, ry, rz;
             const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
             return t != s && r2 < h2 && !(r2 < skip);
         };
-        // wavelet sums (3) and wavelet-weighted velocities (3) of a pair
-        auto pair = [&](int o, uint32_t t, float (&term)[6]) {
-            const float4 po = own_pos[wib][o];
-            const int lko = c.energy_large_kernel ? 0 : lv(po.w);
-            const float ho = c.kernel[lko];
-            const float ih = 1.0f / ho, isq = 1.0f / sqrtf(ho);
+        // the wavelet transform of one neighbour
+        auto pair = [&](uint32_t t) {
             const float4 pj = w.spos_n[t];
             const float4 vj = w.svel_n[t];
             float rx, ry, rz;
-            r2_of<DIM>(po, pj, rx, ry, rz);
+            r2_of<DIM>(pi, pj, rx, ry, rz);
             const float wx = wavelet(rx * ih, amp), wy = wavelet(ry * ih, amp);
-            term[0] = wx; term[1] = wy;
-            term[3] = vj.x * wx * isq; term[4] = vj.y * wy * isq;
+            tsx += wx; tsy += wy;
+            tvx += vj.x * wx * isq; tvy += vj.y * wy * isq;
             if (DIM == 3) {
                 const float wz = wavelet(rz * ih, amp);
-                term[2] = wz;
-                term[5] = vj.z * wz * isq;
+                tsz += wz;
+                tvz += vj.z * wz * isq;
             }
         };
-        float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        warp_pairs<DIM, 6>(c, w.cell_off, w.spos_n, valid, q, smem[wib], acc, accept, pair);
+        warp_pairs<DIM>(c, w.cell_off, w.spos_n, valid, q, smem[wib], accept, pair);
         if (!valid) continue;
-        float tsx = acc[0], tsy = acc[1], tsz = acc[2], tvx = acc[3], tvy = acc[4], tvz = acc[5];
         tvx /= tsx; tvy /= tsy; tvz = DIM == 3 ? tvz / tsz : 0.f;
         float energy = 0.5f * (tvx * tvx + tvy * tvy);
         if (c.energy_mass_weight) energy *= c.mass[li];
