@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(BS) k_reorder(const Counters *__restrict__ cnt
 // order.  Flushing together keeps the expensive pair math converged (lists
 // fill at similar rates, so few lanes idle in a round), and every particle's
 // sums take the same order whichever particles share its warp.
-constexpr uint32_t kWarpCap = 24;             // list fill that triggers a warp flush
+constexpr uint32_t kWarpCap = 40;             // list fill that triggers a warp flush (44 x 32 x 4 B per warp)
 constexpr uint32_t kWarpSlot = kWarpCap + 4;  // a step can add 4 more before the check
 
 struct WarpPairSmem {
