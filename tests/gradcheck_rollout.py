@@ -108,6 +108,11 @@ def main():
     d = np.array(dirs)
     rel_gpu = np.abs(d[:, 0] - d[:, 2]) / np.abs(d[:, 2])
     rel_64 = np.abs(d[:, 1] - d[:, 2]) / np.abs(d[:, 2])
+    # the same errors against the gradient's norm (directions are unit
+    # vectors, so a direction nearly orthogonal to the gradient has a small
+    # |fd| and an inflated relative error)
+    gnorm = float(np.sqrt((g64["d_vel0"] ** 2).sum() + g64["d_mu"] ** 2 + g64["d_k"] ** 2))
+    nrm_gpu = np.abs(d[:, 0] - d[:, 2]) / gnorm
     out = {
         "workload": f"{a.block}^3 block, {a.steps} steps, checkpoints every {a.every}, 32^3 grid loss",
         "particles_initial": len(pos), "particles_final": n_final,
@@ -125,6 +130,8 @@ def main():
         "dir_rel_gpu_vs_fd_max": float(rel_gpu.max()), "dir_rel_gpu_vs_fd_median": float(np.median(rel_gpu)),
         "dir_rel_fp64_adjoint_vs_fd_max": float(rel_64.max()),
         "dirs_within_1e-3": int((np.abs(d[:, 0] - d[:, 2]) <= 1e-3 * np.abs(d[:, 2]) + noise).sum()),
+        "dir_err_over_grad_norm_max": float(nrm_gpu.max()),
+        "dir_abs_fd_over_grad_norm_min": float(np.abs(d[:, 2]).min() / gnorm),
         "seconds": {"gpu_forward_backward": t_gpu, "fp64_adjoint": t_ref, "fp64_fd": t_fd},
         "omp_threads": O.get_threads(),
     }
