@@ -387,6 +387,12 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
         // pairs with r^2 < max(h_i^2, h_j^2) and r^2 >= close_r2 (:797-804)
         const float cut0 = fmaxf(hi2, c.kernel2[0]), cut1 = fmaxf(hi2, c.kernel2[1]);
         const float close = c.close_r2;
+        // neighbour-level constants, once per particle instead of per pair
+        const float jspk0 = c.kernel_h6_twice ? c.spiky[0] / c.kernel6[0] : c.spiky[0];
+        const float jspk1 = c.kernel_h6_twice ? c.spiky[1] / c.kernel6[1] : c.spiky[1];
+        const float jvis0 = c.kernel_h6_twice ? c.visco[0] / c.kernel6[0] : c.visco[0];
+        const float jvis1 = c.kernel_h6_twice ? c.visco[1] / c.kernel6[1] : c.visco[1];
+        const float mimj0 = mi * c.mass[0], mimj1 = mi * c.mass[1];
         auto accept = [&](uint32_t t, const float4 &pj) {
             float rx, ry, rz;
             const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
@@ -414,13 +420,10 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
             }
             const float jkr = __fsub_rn(c.kernel[lj], r);
             if (jkr > 0.0f) {
-                const float jspk = c.kernel_h6_twice ? c.spiky[lj] / c.kernel6[lj] : c.spiky[lj];
-                const float jvis = c.kernel_h6_twice ? c.visco[lj] / c.kernel6[lj] : c.visco[lj];
-                jpk = jspk * jkr * jkr;
-                jvk = jvis * jkr;
+                jpk = (lj ? jspk1 : jspk0) * jkr * jkr;
+                jvk = (lj ? jvis1 : jvis0) * jkr;
             }
-            const float mj = c.mass[lj];
-            const float tp = mi * mj * (ai.z + aj.z) * (ipk + jpk) * 0.5f / r;
+            const float tp = (lj ? mimj1 : mimj0) * (ai.z + aj.z) * (ipk + jpk) * 0.5f / r;
             const float tv = (ai.w * aj.w) * visc * (ivk + jvk) * 0.5f;
             fx += -rx * tp + (evj.x - evi.x) * tv;
             fy += -ry * tp + (evj.y - evi.y) * tv;
