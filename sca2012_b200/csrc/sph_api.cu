@@ -373,6 +373,15 @@ int sph_create(const sph_config *cfg, sph_handle **out)
     rc |= dalloc(h, &w.snbr, cap); rc |= dalloc(h, &w.sinter, cap);
     rc |= dalloc(h, &w.stv, cap); rc |= dalloc(h, &w.sscene, cap);
     rc |= dalloc(h, &w.spos_lo, cap); rc |= dalloc(h, &w.spos_lo_n, cap);
+    // force neighbour lists (256 B per particle of capacity); without them
+    // (very large capacities) the force kernel walks the stencil itself
+    w.flist = nullptr;
+    w.fcnt = nullptr;
+    w.fstride = (uint32_t)cap;
+    if ((uint64_t)cap * kForceListCap * sizeof(uint32_t) <= (8ull << 30)) {
+        rc |= dalloc(h, &w.flist, cap * kForceListCap);
+        rc |= dalloc(h, &w.fcnt, cap);
+    }
     w.pos_comp = cfg->compensated_positions ? 1u : 0u;
     w.scene_tab = nullptr;
     w.nscenes = 0;

@@ -67,7 +67,13 @@ struct WorkPtrs {
     uint32_t *wall;                      // taped steps only: wall contacts per slot
     float4 *spos_lo, *spos_lo_n;         // low position parts per slot (compensated positions)
     uint32_t pos_comp;                   // the config's compensated_positions
+    uint32_t *flist, *fcnt;              // force neighbours per slot, written by the density pass
+    uint32_t fstride;                    // flist[k * fstride + slot]
 };
+
+// Force neighbours the density pass records per particle (more fall back to
+// the force kernel's own stencil walk).
+constexpr uint32_t kForceListCap = 64;
 
 // hi + lo += d with hi, lo FP32 (Fast2Sum; |hi| >= |d + lo| holds for a
 // position and one step's displacement).
@@ -309,17 +315,29 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, const Counters *__
         q.y = (k / c.ncell[0]) % c.ncell[1];
         q.z = DIM == 3 ? k / (c.ncell[0] * c.ncell[1]) : 0u;
         float rho = 0.0f;
-        uint32_t nb = 0;
+        uint32_t nb = 0, nf = 0;
         const float m0 = c.mass[0], m1 = c.mass[1], skip = c.density_skip_r2;
+        // the force pass's neighbours on the way (r^2 < max(h_i^2, h_j^2),
+        // r^2 >= close_r2), in the order its own walk would find them
+        const bool mk = w.flist != nullptr;
+        const float cut0 = fmaxf(h2, c.kernel2[0]), cut1 = fmaxf(h2, c.kernel2[1]);
+        const float close = c.close_r2;
+        const float prune = mk ? fmaxf(cut0, cut1) : h2;
         // single pass: the kernel sum is cheap enough to run predicated
         // (:394-417, j != i with skip <= r^2 < h_i^2)
         auto add = [&](uint32_t t, float4 pj) {
             float dx, dyy, dzz;
             const float r2 = r2_of<DIM>(pj, pi, dx, dyy, dzz);
-            if (t != s && !(r2 < skip) && r2 < h2) {
-                const float x = h2 - r2;
-                rho += (pj.w == 1.0f ? m0 : m1) * poly6 * (x * x * x);
-                ++nb;
+            if (t != s) {
+                if (!(r2 < skip) && r2 < h2) {
+                    const float x = h2 - r2;
+                    rho += (pj.w == 1.0f ? m0 : m1) * poly6 * (x * x * x);
+                    ++nb;
+                }
+                if (mk && r2 < (pj.w == 1.0f ? cut0 : cut1) && !(r2 < close)) {
+                    if (nf < kForceListCap) w.flist[(size_t)nf * w.fstride + s] = t;
+                    ++nf;
+                }
             }
         };
 #pragma unroll 1
@@ -327,7 +345,7 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, const Counters *__
 #pragma unroll 1
             for (int dy = -1; dy <= 1; ++dy) {
                 uint32_t b, e;
-                if (!row_range_pruned<DIM>(c, w.cell_off, q, pi, h2, dy, dz, b, e)) continue;
+                if (!row_range_pruned<DIM>(c, w.cell_off, q, pi, prune, dy, dz, b, e)) continue;
                 uint32_t t = b;
                 for (; t + 4 <= e; t += 4) {
                     const float4 p0 = w.spos[t], p1 = w.spos[t + 1], p2 = w.spos[t + 2], p3 = w.spos[t + 3];
@@ -344,6 +362,7 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, const Counters *__
         float p = (r * r * r - 1.0f) * gas;
         w.saux[s] = make_float4(rho, p, p / (rho * rho), c.mass[li] / rho);
         w.snbr[s] = nb;
+        if (mk) w.fcnt[s] = nf;
     }
 }
 
@@ -429,7 +448,16 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
             fy += -ry * tp + (evj.y - evi.y) * tv;
             if (DIM == 3) fz += -rz * tp + (evj.z - evi.z) * tv;
         };
-        warp_pairs<DIM>(c, w.cell_off, w.spos, valid, q, smem[wib], accept, pair);
+        const unsigned full = 0xffffffffu;
+        const uint32_t nf = valid && w.flist ? w.fcnt[s] : 0u;
+        if (__all_sync(full, w.flist != nullptr && nf <= kForceListCap)) {
+            // the density pass's list: same neighbours, same order as the walk
+            const uint32_t m = __reduce_max_sync(full, nf);
+            for (uint32_t kk = 0; kk < m; ++kk)
+                if (kk < nf) pair(w.flist[(size_t)kk * w.fstride + s]);
+        } else {
+            warp_pairs<DIM>(c, w.cell_off, w.spos, valid, q, smem[wib], accept, pair);
+        }
         if (!valid) continue;
         // surface tension switch (SPH-3D-2/sph_system.cu:1113-1136)
         const float nrm = sqrtf(gx * gx + gy * gy + gz * gz);
