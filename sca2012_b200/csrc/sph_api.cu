@@ -377,7 +377,6 @@ int sph_create(const sph_config *cfg, sph_handle **out)
     // (very large capacities) the force kernel walks the stencil itself
     w.flist = nullptr;
     w.fcnt = nullptr;
-    w.fstride = (uint32_t)cap;
     if ((uint64_t)cap * kForceListCap * sizeof(uint32_t) <= (8ull << 30)) {
         rc |= dalloc(h, &w.flist, cap * kForceListCap);
         rc |= dalloc(h, &w.fcnt, cap);

@@ -67,8 +67,7 @@ struct WorkPtrs {
     uint32_t *wall;                      // taped steps only: wall contacts per slot
     float4 *spos_lo, *spos_lo_n;         // low position parts per slot (compensated positions)
     uint32_t pos_comp;                   // the config's compensated_positions
-    uint32_t *flist, *fcnt;              // force neighbours per slot, written by the density pass
-    uint32_t fstride;                    // flist[k * fstride + slot]
+    uint32_t *flist, *fcnt;              // force neighbours: flist[slot * kForceListCap + k], by the density pass
 };
 
 // Force neighbours the density pass records per particle (more fall back to
@@ -335,8 +334,8 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, const Counters *__
                     ++nb;
                 }
                 if (mk && r2 < (pj.w == 1.0f ? cut0 : cut1) && !(r2 < close)) {
-                    if (nf < kForceListCap) w.flist[(size_t)nf * w.fstride + s] = t;
-                    ++nf;
+                    if (nf < kForceListCap) w.flist[(size_t)s * kForceListCap + nf] = t;   // a particle's
+                    ++nf;                                                                   // entries share sectors
                 }
             }
         };
@@ -453,8 +452,9 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
         if (__all_sync(full, w.flist != nullptr && nf <= kForceListCap)) {
             // the density pass's list: same neighbours, same order as the walk
             const uint32_t m = __reduce_max_sync(full, nf);
+            const uint32_t *mine = w.flist + (size_t)s * kForceListCap;
             for (uint32_t kk = 0; kk < m; ++kk)
-                if (kk < nf) pair(w.flist[(size_t)kk * w.fstride + s]);
+                if (kk < nf) pair(mine[kk]);
         } else {
             warp_pairs<DIM>(c, w.cell_off, w.spos, valid, q, smem[wib], accept, pair);
         }
