@@ -418,10 +418,7 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
             return t != s && r2 < cut && !(r2 < close);
         };
         // pressure, viscosity and colour-field terms of one neighbour
-        auto pair = [&](uint32_t t) {
-            const float4 pj = w.spos[t];
-            const float4 aj = w.saux[t];
-            const float4 evj = w.sev[t];
+        auto pair_with = [&](const float4 pj, const float4 aj, const float4 evj) {
             float rx, ry, rz;
             const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
             const int lj = lv(pj.w);
@@ -447,13 +444,32 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
             fy += -ry * tp + (evj.y - evi.y) * tv;
             if (DIM == 3) fz += -rz * tp + (evj.z - evi.z) * tv;
         };
+        auto pair = [&](uint32_t t) { pair_with(w.spos[t], w.saux[t], w.sev[t]); };
         const unsigned full = 0xffffffffu;
         const uint32_t nf = valid && w.flist ? w.fcnt[s] : 0u;
         if (__all_sync(full, w.flist != nullptr && nf <= kForceListCap)) {
             // the density pass's list: same neighbours, same order as the walk
             const uint32_t m = __reduce_max_sync(full, nf);
             const uint32_t *mine = w.flist + (size_t)s * kForceListCap;
-            for (uint32_t kk = 0; kk < m; ++kk)
+            uint32_t kk = 0;
+            // four entries per 16-byte load, their neighbours' loads issued
+            // before the math (entries past nf are replaced by the particle itself)
+            for (; kk + 4 <= m; kk += 4) {
+                const uint4 t4 = *reinterpret_cast<const uint4 *>(mine + kk);
+                const uint32_t tt[4] = {kk < nf ? t4.x : s, kk + 1 < nf ? t4.y : s, kk + 2 < nf ? t4.z : s,
+                                        kk + 3 < nf ? t4.w : s};
+                float4 pj[4], aj[4], ej[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    pj[u] = w.spos[tt[u]];
+                    aj[u] = w.saux[tt[u]];
+                    ej[u] = w.sev[tt[u]];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (kk + u < nf) pair_with(pj[u], aj[u], ej[u]);
+            }
+            for (; kk < m; ++kk)
                 if (kk < nf) pair(mine[kk]);
         } else {
             warp_pairs<DIM>(c, w.cell_off, w.spos, valid, q, smem[wib], accept, pair);
