@@ -240,18 +240,30 @@ __global__ void __launch_bounds__(BS) k_reorder(const Counters *__restrict__ cnt
 constexpr uint32_t kWarpCap = 40;             // list fill that triggers a warp flush (44 x 32 x 4 B per warp)
 constexpr uint32_t kWarpSlot = kWarpCap + 4;  // a step can add 4 more before the check
 
+struct NbrPV { float4 p, v; };       // position, velocity
+
+// Bundles a fetch(t) and a use(fetched) callable for warp_pairs<.., AHEAD>.
+template <class F, class U> struct FetchUse {
+    F fetch;
+    U use;
+};
+template <class F, class U> __device__ __forceinline__ FetchUse<F, U> fetch_use(F f, U u) { return {f, u}; }
+
 struct WarpPairSmem {
     uint32_t lst[kWarpSlot][32];     // per-lane lists, entry-major (appends hit 32 banks)
 };
 
 // accept(t, pj): this lane's test of candidate slot t at position pj.
 // pair(t): adds this lane's pair with neighbour slot t into its sums.
-// Every lane of the warp must call it (active = false for a lane without a
-// particle).
-template <int DIM, class Accept, class Pair>
+// AHEAD > 0: pair is instead a fetch(t) / use(fetched) pair of callables
+// (FetchUse) and a flush fetches AHEAD pairs before their math (entries past
+// the lane's list read slot `self`), for callers whose fetched data fits in
+// registers.  Every lane of the warp must call it (active = false for a lane
+// without a particle).
+template <int DIM, int AHEAD = 0, class Accept, class Pair>
 __device__ __forceinline__ void warp_pairs(const sph_config &c, const uint32_t *__restrict__ off,
                                            const float4 *__restrict__ pos, bool active, uint3 q,
-                                           WarpPairSmem &sm, Accept accept, Pair pair)
+                                           WarpPairSmem &sm, Accept accept, Pair pair, uint32_t self = 0)
 {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -273,8 +285,22 @@ __device__ __forceinline__ void warp_pairs(const sph_config &c, const uint32_t *
     uint32_t cnt = 0;
     auto flush = [&]() {
         const uint32_t m = __reduce_max_sync(full, cnt);
-        for (uint32_t k = 0; k < m; ++k)
-            if (k < cnt) pair(sm.lst[k][lane]);
+        if constexpr (AHEAD == 0) {
+            for (uint32_t k = 0; k < m; ++k)
+                if (k < cnt) pair(sm.lst[k][lane]);
+        } else {
+            uint32_t k = 0;
+            for (; k + AHEAD <= m; k += AHEAD) {
+                decltype(pair.fetch(self)) got[AHEAD];
+#pragma unroll
+                for (int u = 0; u < AHEAD; ++u) got[u] = pair.fetch(k + u < cnt ? sm.lst[k + u][lane] : self);
+#pragma unroll
+                for (int u = 0; u < AHEAD; ++u)
+                    if (k + u < cnt) pair.use(got[u]);
+            }
+            for (; k < m; ++k)
+                if (k < cnt) pair.use(pair.fetch(sm.lst[k][lane]));
+        }
         cnt = 0;
         __syncwarp();
     };
@@ -619,10 +645,10 @@ __global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counter
             const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
             return t != s && r2 < h2 && !(r2 < skip);
         };
-        // the wavelet transform of one neighbour
-        auto pair = [&](uint32_t t) {
-            const float4 pj = w.spos_n[t];
-            const float4 vj = w.svel_n[t];
+        // the wavelet transform of one neighbour (its loads fetched ahead)
+        auto fetch = [&](uint32_t t) { return NbrPV{w.spos_n[t], w.svel_n[t]}; };
+        auto use = [&](const NbrPV &g) {
+            const float4 pj = g.p, vj = g.v;
             float rx, ry, rz;
             r2_of<DIM>(pi, pj, rx, ry, rz);
             const float wx = wavelet(rx * ih, amp), wy = wavelet(ry * ih, amp);
@@ -634,7 +660,7 @@ __global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counter
                 tvz += vj.z * wz * isq;
             }
         };
-        warp_pairs<DIM>(c, w.cell_off, w.spos_n, valid, q, smem[wib], accept, pair);
+        warp_pairs<DIM, 4>(c, w.cell_off, w.spos_n, valid, q, smem[wib], accept, fetch_use(fetch, use), s);
         if (!valid) continue;
         tvx /= tsx; tvy /= tsy; tvz = DIM == 3 ? tvz / tsz : 0.f;
         float energy = 0.5f * (tvx * tvx + tvy * tvy);
