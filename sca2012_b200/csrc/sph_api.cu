@@ -1055,7 +1055,7 @@ namespace {
 
 bool tune_valid(int st, uint32_t bs, uint32_t bpsm, uint32_t cap)
 {
-    const bool listed = st == SPH_TUNE_FORCE || st == SPH_TUNE_ENERGY;   // the two-phase list kernels
+    const bool listed = st == SPH_TUNE_FORCE || st == SPH_TUNE_ENERGY;   // kernels with shared-memory lists
     return (bs == 128 || bs == 256 || (bs == 512 && !listed)) && bpsm >= 1 && bpsm <= 64 && cap <= 1 &&
            (st == SPH_TUNE_FORCE || cap == 0);
 }
