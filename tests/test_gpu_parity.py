@@ -35,6 +35,8 @@ CASES = {
     "dam_3d2_small": (sph.PRESET_DAM_3D2, lambda c: scenes.block_3d(c, (24, 24, 12), 0.01, seed=3), 3),
     "ref_3d2_obstacles": (sph.PRESET_REF_3D2, scenes.ref_box_3d2, 8, _obstacles),
     "ref_2d_mouse": (sph.PRESET_REF_2D, scenes.ref_init_2d, 10, _mouse),
+    # the benchmark workload at full size: 1,114,112 particles, four-way
+    "dam_3d4_full": (sph.PRESET_DAM_3D4, scenes.dam_3d4, 2),
 }
 
 
