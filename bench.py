@@ -471,6 +471,13 @@ def batched_scenes(args, rank=0, world=1):
         particles += len(pos)
     timed(bs, 3)
     t_batched = timed(bs, steps)
+    # the same steps with plain launches: what graph replay saves, i.e. the
+    # launch overhead a single persistent launch per step could remove at most
+    for h in bs:
+        h.set_graph(False)
+    t_eager = timed(bs, steps)
+    for h in bs:
+        h.set_graph(True)
     status = 0
     if world > 1:
         n_mine = sum(len(b[1]) for b in batches)
@@ -525,7 +532,8 @@ def batched_scenes(args, rank=0, world=1):
             "batched_scene_steps_per_s": v_b, "sequential_scene_steps_per_s": v_s,
             "concurrent_streams_scene_steps_per_s": v_c,
             "batched_vs_sequential": v_b / v_s, "batched_vs_concurrent_streams": v_b / v_c,
-            "batched_ms_per_step": t_batched / steps * 1e3, "status": status,
+            "batched_ms_per_step": t_batched / steps * 1e3,
+            "batched_eager_launches_ms_per_step": t_eager / steps * 1e3, "status": status,
             "adjoint_last_50": {"forward_ms_per_step": t_fwd / adj_steps * 1e3,
                                 "backward_ms_per_step": t_bwd / adj_steps * 1e3,
                                 "backward_vs_forward": t_bwd / t_fwd,

@@ -4,10 +4,13 @@
 //   canonical state, two buffers swapped every step, in the reference's
 //   particle-index order (the order split/merge/compaction and the readback
 //   depend on): pos4 = (x, y, z, level), vel4, ev4, acc4, dens, press,
-//   energy, surface, interior;
+//   energy, surface, interior, and when in use scene (batched scenes) and
+//   pos_lo (compensated positions);
 //   sorted working copies, in cell-key order, that the neighbour loops read
 //   contiguously: spos/svel/sev (gathered), saux = (rho, p, p/rho^2, m/rho),
-//   and the post-integration spos_n/svel_n/sev_n/sacc_n, ssurf, senergy.
+//   and the post-integration spos_n/svel_n/sev_n/sacc_n, ssurf, senergy;
+//   per-particle force-neighbour lists (flist), written by the density pass
+//   and read by the force pass.
 // Cell key = z*R*C + y*R + x with x = floor(pos / cell) in FP32, exactly the
 // reference's calc_grid_pos/calc_grid_hash (SPH-3D-2/sph_system.cu:18-32).
 // Neighbour search visits the 3 (2D) or 9 (3D) rows of x-adjacent cells; in
