@@ -146,6 +146,9 @@ typedef struct sph_config {
     float close_r2;          /* the force loop (and the energy loop with energy_skip_close) skips
                                 pairs with r^2 below this: reference 1e-4, a constant of its unit
                                 system (SPH-3D-2/sph_system.cu:801-804, SPH-2D/sph_system.cu:584) */
+    uint32_t walk_only;      /* 1: the force and energy passes walk the cell stencil themselves
+                                instead of reading the neighbour lists the density pass records
+                                (same pairs, same order, same results; a comparison switch) */
 } sph_config;
 
 /* Host view of a particle state (SoA).  Vectors hold `dim` floats per
@@ -415,8 +418,9 @@ int sph_conserved(sph_handle *h, double out[7]);
 typedef struct sph_tuning {
     uint32_t block[SPH_TUNE_STAGES];
     uint32_t blocks_per_sm[SPH_TUNE_STAGES];   /* 1..64 */
-    uint32_t reg_cap[SPH_TUNE_STAGES];         /* force: 1 = register-capped build (8 blocks of 128 or 4
-                                                  of 256 resident per SM, 64 registers); 0 elsewhere */
+    uint32_t reg_cap[SPH_TUNE_STAGES];         /* force and energy: 1 = register-capped build (8 blocks
+                                                  of 128 or 4 of 256 resident per SM, 64 registers);
+                                                  0 elsewhere */
     float step_ms_before, step_ms_after;       /* sph_autotune: mean step time before / after */
 } sph_tuning;
 

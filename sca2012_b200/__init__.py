@@ -238,11 +238,14 @@ class Solver:
         return self._tuning_dict(t)
 
     def set_tuning(self, block, blocks_per_sm, reg_cap=None):
+        """reg_cap None keeps the handle's register caps."""
+        if reg_cap is None:
+            reg_cap = self.get_tuning()["reg_cap"]
         t = _abi.Tuning()
         for k in range(_abi.TUNE_STAGES):
             t.block[k] = int(block[k])
             t.blocks_per_sm[k] = int(blocks_per_sm[k])
-            t.reg_cap[k] = int(reg_cap[k]) if reg_cap is not None else 0
+            t.reg_cap[k] = int(reg_cap[k])
         self._check(self._lib.sph_set_tuning(self._h, C.byref(t)), "sph_set_tuning")
 
     @staticmethod

@@ -64,6 +64,7 @@ class Config(C.Structure):
         ("dens_mul", C.c_uint32), ("den_size", C.c_float), ("ndens", U3), ("iso_value", C.c_float),
         ("mc_interpolate", C.c_uint32), ("splat_with_kernel", C.c_uint32), ("grid_every", C.c_uint32),
         ("max_triangles", C.c_uint32), ("compensated_positions", C.c_uint32), ("close_r2", C.c_float),
+        ("walk_only", C.c_uint32),
     ]
 
     def copy(self):

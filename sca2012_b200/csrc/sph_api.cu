@@ -79,7 +79,7 @@ struct sph_handle {
     double *cons = nullptr;   // conserved-quantity partial sums (allocated on first use)
     uint32_t tune_bs[SPH_TUNE_STAGES] = {256, 256, 256, 256, 256, 256, 256, 256};
     uint32_t tune_bpsm[SPH_TUNE_STAGES] = {8, 8, 8, 8, 8, 8, 8, 8};
-    uint32_t tune_minb[SPH_TUNE_STAGES] = {0, 0, 0, 0, 0, 0, 0, 0};   // 1: register-capped variant
+    uint32_t tune_minb[SPH_TUNE_STAGES] = {0, 0, 0, 0, 0, 1, 0, 0};   // 1: register-capped variant
 };
 
 namespace {
@@ -220,6 +220,9 @@ template <int DIM> int run_step(sph_handle *h)
     CanonPtrs in = h->buf[p], out = h->buf[p ^ 1];
     h->w.pos_comp = c.compensated_positions ? 1u : 0u;
     WorkPtrs w = h->w;
+    if (c.walk_only) {   // the same pairs found by the stencil walks
+        w.nlist = w.ncnt = nullptr;
+    }
     cudaStream_t s = h->stream;
     h->nstages = 0;
     if (h->profiling) cudaEventRecord(h->ev[0], s);
@@ -252,7 +255,7 @@ template <int DIM> int run_step(sph_handle *h)
         h->grid_valid = true;
         stage(h, "surface");
     }
-    SPH_BS_SWITCH2(h->tune_bs[SPH_TUNE_ENERGY], 1,   // 64 registers fit without spills
+    SPH_BS_SWITCH2(h->tune_bs[SPH_TUNE_ENERGY], h->tune_minb[SPH_TUNE_ENERGY],
                    k_energy_split<DIM, B, M><<<grid_st(h, nub, SPH_TUNE_ENERGY), B, 0, s>>>(c, cin, in, w,
                                                                                           h->debug ? 1 : 0));
     stage(h, "energy_split");
@@ -373,13 +376,14 @@ int sph_create(const sph_config *cfg, sph_handle **out)
     rc |= dalloc(h, &w.snbr, cap); rc |= dalloc(h, &w.sinter, cap);
     rc |= dalloc(h, &w.stv, cap); rc |= dalloc(h, &w.sscene, cap);
     rc |= dalloc(h, &w.spos_lo, cap); rc |= dalloc(h, &w.spos_lo_n, cap);
-    // force neighbour lists (256 B per particle of capacity); without them
-    // (very large capacities) the force kernel walks the stencil itself
-    w.flist = nullptr;
-    w.fcnt = nullptr;
-    if ((uint64_t)cap * kForceListCap * sizeof(uint32_t) <= (8ull << 30)) {
-        rc |= dalloc(h, &w.flist, cap * kForceListCap);
-        rc |= dalloc(h, &w.fcnt, cap);
+    // neighbour candidate lists (512 B per particle of capacity); without
+    // them (very large capacities) the force and energy kernels walk the
+    // stencil themselves
+    w.nlist = nullptr;
+    w.ncnt = nullptr;
+    if ((uint64_t)cap * kNbrListCap * sizeof(uint32_t) <= (12ull << 30)) {
+        rc |= dalloc(h, &w.nlist, cap * kNbrListCap);
+        rc |= dalloc(h, &w.ncnt, cap);
     }
     w.pos_comp = cfg->compensated_positions ? 1u : 0u;
     w.scene_tab = nullptr;
@@ -1057,7 +1061,7 @@ bool tune_valid(int st, uint32_t bs, uint32_t bpsm, uint32_t cap)
 {
     const bool listed = st == SPH_TUNE_FORCE || st == SPH_TUNE_ENERGY;   // kernels with shared-memory lists
     return (bs == 128 || bs == 256 || (bs == 512 && !listed)) && bpsm >= 1 && bpsm <= 64 && cap <= 1 &&
-           (st == SPH_TUNE_FORCE || cap == 0);
+           (st == SPH_TUNE_FORCE || st == SPH_TUNE_ENERGY || cap == 0);
 }
 
 const char *const kTuneStageName[SPH_TUNE_STAGES] = {"hash", "scatter", "reorder", "density",

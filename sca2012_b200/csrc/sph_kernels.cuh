@@ -9,8 +9,8 @@
 //   sorted working copies, in cell-key order, that the neighbour loops read
 //   contiguously: spos/svel/sev (gathered), saux = (rho, p, p/rho^2, m/rho),
 //   and the post-integration spos_n/svel_n/sev_n/sacc_n, ssurf, senergy;
-//   per-particle force-neighbour lists (flist), written by the density pass
-//   and read by the force pass.
+//   per-particle neighbour candidate lists (nlist), written by the density
+//   pass and read by the force and energy passes.
 // Cell key = z*R*C + y*R + x with x = floor(pos / cell) in FP32, exactly the
 // reference's calc_grid_pos/calc_grid_hash (SPH-3D-2/sph_system.cu:18-32).
 // Neighbour search visits the 3 (2D) or 9 (3D) rows of x-adjacent cells; in
@@ -36,7 +36,8 @@ struct Counters {
     uint32_t n_removed;    // merged-away particles this step
     uint32_t error;        // SPH_ERR_* bit flags (1 << code)
     uint32_t split_off;    // 1: splits suppressed this step (capacity)
-    uint32_t pad[3];
+    uint32_t disp2_max;    // bits of the step's largest squared displacement (FP32 >= 0), by the force pass
+    uint32_t pad[2];
 };
 
 struct CanonPtrs {
@@ -70,12 +71,37 @@ struct WorkPtrs {
     uint32_t *wall;                      // taped steps only: wall contacts per slot
     float4 *spos_lo, *spos_lo_n;         // low position parts per slot (compensated positions)
     uint32_t pos_comp;                   // the config's compensated_positions
-    uint32_t *flist, *fcnt;              // force neighbours: flist[slot * kForceListCap + k], by the density pass
+    uint32_t *nlist, *ncnt;              // neighbour candidates: nlist[slot * kNbrListCap + k], by the density pass
 };
 
-// Force neighbours the density pass records per particle (more fall back to
-// the force kernel's own stencil walk).
-constexpr uint32_t kForceListCap = 64;
+// Neighbour candidates the density pass records per particle: every stencil
+// neighbour within (1 + kNbrListMargin) h_max of the start-of-step position,
+// in stencil-walk order (more than kNbrListCap: the consumers walk).
+//  - The force pass uses the same positions: filtering the list with its own
+//    test (r^2 < max(h_i^2, h_j^2), r^2 >= close_r2) gives its walk's pairs
+//    in its walk's order.
+//  - The energy pass tests the particles' integrated positions against the
+//    stale cell lists of the particle's NEW cell.  When that cell is the old
+//    one and |d_i| + max_j |d_j| (d: the step's displacements) stays under
+//    the margin, every pair it accepts has a start-of-step distance below
+//    h + margin, so it is on the list: filtering the list gives the walk's
+//    pairs in the walk's order.  Other particles walk the stencil.
+// Either way the sums are those of the walk, bit for bit.
+constexpr uint32_t kNbrListCap = 128;
+constexpr float kNbrListMargin = 0.05f;
+
+__device__ __forceinline__ float energy_list_r2(const sph_config &c)
+{
+    const float r = 1.0f + kNbrListMargin;
+    return fmaxf(c.kernel2[0], c.kernel2[1]) * (r * r);
+}
+
+// the displacement budget the list covers: 1% under the margin, far above
+// the FP32 rounding of the distances involved (~1e-7 relative)
+__device__ __forceinline__ float energy_list_budget(const sph_config &c)
+{
+    return 0.99f * kNbrListMargin * sqrtf(fmaxf(c.kernel2[0], c.kernel2[1]));
+}
 
 // hi + lo += d with hi, lo FP32 (Fast2Sum; |hi| >= |d + lo| holds for a
 // position and one step's displacement).
@@ -329,9 +355,10 @@ __device__ __forceinline__ void warp_pairs(const sph_config &c, const uint32_t *
 // rho_i = m_i poly6_i h_i^6 + sum_{j != i, skip <= r^2 < h_i^2} m_j poly6_i (h_i^2 - r^2)^3
 // p_i = k ((rho_i / rho0)^3 - 1)         (SPH-3D-2/sph_system.cu:338-677)
 template <int DIM, int BS = kThreads>
-__global__ void __launch_bounds__(BS) k_density(sph_config c, const Counters *__restrict__ cnt, WorkPtrs w)
+__global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restrict__ cnt, WorkPtrs w)
 {
     const uint32_t n = cnt->n;
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt->disp2_max = 0u;   // the force pass takes the max
     for (uint32_t s = grid_stride_start(); s < n; s += grid_stride()) {
         const float4 pi = w.spos[s];
         const int li = lv(pi.w);
@@ -343,14 +370,14 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, const Counters *__
         q.y = (k / c.ncell[0]) % c.ncell[1];
         q.z = DIM == 3 ? k / (c.ncell[0] * c.ncell[1]) : 0u;
         float rho = 0.0f;
-        uint32_t nb = 0, nf = 0;
+        uint32_t nb = 0, nl = 0;
         const float m0 = c.mass[0], m1 = c.mass[1], skip = c.density_skip_r2;
-        // the force pass's neighbours on the way (r^2 < max(h_i^2, h_j^2),
-        // r^2 >= close_r2), in the order its own walk would find them
-        const bool mk = w.flist != nullptr;
-        const float cut0 = fmaxf(h2, c.kernel2[0]), cut1 = fmaxf(h2, c.kernel2[1]);
-        const float close = c.close_r2;
-        const float prune = mk ? fmaxf(cut0, cut1) : h2;
+        // the force and energy passes' candidates on the way
+        // (r^2 < (1 + margin)^2 h_max^2), in the order their walks find them
+        const bool rec = w.nlist != nullptr;
+        const float re2 = energy_list_r2(c);
+        const float prune = rec ? fmaxf(re2, h2) : h2;
+        uint32_t *mine = rec ? w.nlist + (size_t)s * kNbrListCap : nullptr;   // a particle's entries share sectors
         // single pass: the kernel sum is cheap enough to run predicated
         // (:394-417, j != i with skip <= r^2 < h_i^2)
         auto add = [&](uint32_t t, float4 pj) {
@@ -362,9 +389,9 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, const Counters *__
                     rho += (pj.w == 1.0f ? m0 : m1) * poly6 * (x * x * x);
                     ++nb;
                 }
-                if (mk && r2 < (pj.w == 1.0f ? cut0 : cut1) && !(r2 < close)) {
-                    if (nf < kForceListCap) w.flist[(size_t)s * kForceListCap + nf] = t;   // a particle's
-                    ++nf;                                                                   // entries share sectors
+                if (rec && r2 < re2) {
+                    if (nl < kNbrListCap) mine[nl] = t;
+                    ++nl;
                 }
             }
         };
@@ -390,7 +417,7 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, const Counters *__
         float p = (r * r * r - 1.0f) * gas;
         w.saux[s] = make_float4(rho, p, p / (rho * rho), c.mass[li] / rho);
         w.snbr[s] = nb;
-        if (mk) w.fcnt[s] = nf;
+        if (rec) w.ncnt[s] = nl;
     }
 }
 
@@ -475,11 +502,12 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
         };
         auto pair = [&](uint32_t t) { pair_with(w.spos[t], w.saux[t], w.sev[t]); };
         const unsigned full = 0xffffffffu;
-        const uint32_t nf = valid && w.flist ? w.fcnt[s] : 0u;
-        if (__all_sync(full, w.flist != nullptr && nf <= kForceListCap)) {
-            // the density pass's list: same neighbours, same order as the walk
+        const uint32_t nf = valid && w.nlist ? w.ncnt[s] : 0u;
+        if (__all_sync(full, w.nlist != nullptr && nf <= kNbrListCap)) {
+            // the density pass's candidates, filtered by the walk's test: same
+            // neighbours, same order as the walk
             const uint32_t m = __reduce_max_sync(full, nf);
-            const uint32_t *mine = w.flist + (size_t)s * kForceListCap;
+            const uint32_t *mine = w.nlist + (size_t)s * kNbrListCap;
             uint32_t kk = 0;
             // four entries per 16-byte load, their neighbours' loads issued
             // before the math (entries past nf are replaced by the particle itself)
@@ -496,10 +524,14 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
-                    if (kk + u < nf) pair_with(pj[u], aj[u], ej[u]);
+                    if (kk + u < nf && accept(tt[u], pj[u])) pair_with(pj[u], aj[u], ej[u]);
             }
             for (; kk < m; ++kk)
-                if (kk < nf) pair(mine[kk]);
+                if (kk < nf) {
+                    const uint32_t t = mine[kk];
+                    const float4 pj = w.spos[t];
+                    if (accept(t, pj)) pair_with(pj, w.saux[t], w.sev[t]);
+                }
         } else {
             warp_pairs<DIM>(c, w.cell_off, w.spos, valid, q, smem[wib], accept, pair);
         }
@@ -607,6 +639,16 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
         w.svel_n[s] = v;
         w.sev_n[s] = ev;
         w.sacc_n[s] = a;
+        if (w.nlist) {   // the step's largest squared displacement, one atomic per group of lanes
+            float ddx, ddy, ddz;
+            const float d2 = r2_of<DIM>(x, pi, ddx, ddy, ddz);
+            // non-negative floats order as their bits; a NaN position (which
+            // passes no neighbour test) is left out
+            const uint32_t bits = d2 == d2 ? __float_as_uint(d2) : 0u;
+            const unsigned am = __activemask();
+            const uint32_t m = __reduce_max_sync(am, bits);
+            if (lane == __ffs(am) - 1) atomicMax(&cnt->disp2_max, m);
+        }
     }
 }
 
@@ -630,6 +672,9 @@ __global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counter
     // 2/(PI^0.25 * sqrt(3 sigma)) with PI = 3.141592f, sigma = 2
     const float amp = 2.0f / (powf(3.141592f, 0.25f) * sqrtf(6.0f));
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    // displacement budget left for this particle's own move (the list covers
+    // |d_i| + max_j |d_j| up to energy_list_budget)
+    const float own_budget = w.nlist ? energy_list_budget(c) - sqrtf(__uint_as_float(cnt->disp2_max)) : -1.0f;
     for (uint32_t base = blockIdx.x * BS + wib * 32u; base < n; base += gridDim.x * BS) {
         const uint32_t s_raw = base + lane;
         const bool valid = s_raw < n;
@@ -663,7 +708,38 @@ __global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counter
                 tvz += vj.z * wz * isq;
             }
         };
-        warp_pairs<DIM, 4>(c, w.cell_off, w.spos_n, valid, q, smem[wib], accept, fetch_use(fetch, use), s);
+        // the density pass's candidates when the particle kept its cell and the
+        // step's moves fit the margin; the stencil walk otherwise
+        // (every test is false for a NaN distance or budget: such a lane walks)
+        uint32_t ne = 0;
+        bool walk = valid;
+        if (valid && own_budget >= 0.0f) {
+            float ddx, ddy, ddz;
+            const float d2 = r2_of<DIM>(pi, w.spos[s], ddx, ddy, ddz);
+            const uint32_t cand = w.ncnt[s];
+            if (cand <= kNbrListCap && key_of(c, q.x, q.y, q.z) == w.skey[s] && sqrtf(d2) <= own_budget) {
+                ne = cand;
+                walk = false;
+            }
+        }
+        const uint32_t m = __reduce_max_sync(0xffffffffu, ne);
+        if (m) {
+            const uint32_t *mine = w.nlist + (size_t)s * kNbrListCap;
+            // four entries per 16-byte load, their neighbours fetched before the
+            // math (entries past ne are replaced by the particle itself)
+            for (uint32_t kk = 0; kk < m; kk += 4) {
+                const uint4 t4 = kk < ne ? *reinterpret_cast<const uint4 *>(mine + kk) : make_uint4(s, s, s, s);
+                const uint32_t tt[4] = {kk < ne ? t4.x : s, kk + 1 < ne ? t4.y : s, kk + 2 < ne ? t4.z : s,
+                                        kk + 3 < ne ? t4.w : s};
+                NbrPV g[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) g[u] = fetch(tt[u]);
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (kk + u < ne && accept(tt[u], g[u].p)) use(g[u]);
+            }
+        }
+        warp_pairs<DIM, 4>(c, w.cell_off, w.spos_n, walk, q, smem[wib], accept, fetch_use(fetch, use), s);
         if (!valid) continue;
         tvx /= tsx; tvy /= tsy; tvz = DIM == 3 ? tvz / tsz : 0.f;
         float energy = 0.5f * (tvx * tvx + tvy * tvy);
