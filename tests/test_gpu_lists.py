@@ -1,11 +1,12 @@
 """Neighbour lists against the stencil walks: the density pass records each
 particle's neighbour candidates (within 1.05 h_max of its start-of-step
 position), and the force and energy passes filter that list instead of
-walking the 3^DIM-cell stencil whenever it holds the walk's pairs.  With walk_only = 1 every pass walks.  Both must
-give the same particles, bit for bit, over many steps with splits and merges:
-at rest (the lists serve almost every particle), with fast random velocities
-(some particles move farther than the lists' margin allows or change cell,
-and walk), and so fast that no list may be used."""
+walking the 3^DIM-cell stencil whenever it holds the walk's pairs.  With
+walk_only = 1 every pass walks.  Both must give the same particles, bit for
+bit, over many steps with splits and merges: at rest (the lists serve almost
+every particle), with fast random velocities (some particles move farther
+than the lists' margin allows or change cell, and walk), and so fast that no
+list may be used."""
 import numpy as np
 import pytest
 
