@@ -853,73 +853,115 @@ template <int DIM, int BS = kThreads>
 __global__ void __launch_bounds__(BS) k_merge(sph_config c, const Counters *__restrict__ cnt,
                                                    CanonPtrs st, WorkPtrs w, uint32_t ncells, uint32_t cap)
 {
-    __shared__ uint32_t list[BS / 32][kMergeListMax];
+    __shared__ uint32_t list[BS / 32][kMergeListMax];    // eligible slots in slot order
+    __shared__ uint32_t lcell[BS / 32][kMergeListMax];   // their cells
+    __shared__ uint8_t lrank[BS / 32][kMergeListMax];    // their ranks among their cell's eligible members
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
     const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
     const uint32_t n = cnt->n;
     const uint32_t split_on = cnt->split_off ? 0u : 1u;
     const uint32_t ways = c.split_ways == 4 ? 4u : 2u;
     const uint32_t extra = ways - 1u;
     const float hs2 = c.kernel[1] / 2.0f;
-    // each warp takes 32 consecutive cells at a time: one lane per cell reads
-    // its member count, and the warp then works only on the cells that hold
-    // enough members to form a group
-    for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + wib) * 32u; base < ncells; base += warps_total * 32u) {
-        const uint32_t mine = base + lane;
-        const uint32_t members = mine < ncells ? w.cell_off[mine + 1] - w.cell_off[mine] : 0u;
-        uint32_t todo = __ballot_sync(0xffffffffu, members >= ways);
-        while (todo) {
-        const uint32_t cell = base + (__ffs(todo) - 1);
-        todo &= todo - 1;
-        const uint32_t b = w.cell_off[cell], e = w.cell_off[cell + 1];
-        // 2D rule: the criterion of the particle whose INDEX equals the cell
-        // index, as memory holds it at merge time (SPH-2D/sph_system.cu:1207)
-        float cell_score = 0.f;
-        if (c.merge_rule == SPH_MERGE_WAVELET_CELL) {
-            float eq, sq;
-            const uint32_t n_after = n + (split_on ? cnt->n_split * extra : 0u);
-            if (cell < n) {
-                const uint32_t sl = w.inv[cell];
-                eq = w.senergy[sl]; sq = w.ssurf[sl];
-            } else if (cell < n_after) {
-                const uint32_t sl = w.inv[w.split_list[(cell - n) / extra]];
-                eq = w.senergy[sl]; sq = w.ssurf[sl];
-            } else if (cell < cap) {
-                eq = st.energy[cell]; sq = st.surface[cell];
-            } else {
-                eq = 0.f; sq = 0.f;   // beyond the allocation: treated as zeroed memory
-            }
-            cell_score = split_score(c, eq, sq);
+    // 2D rule: the criterion of the particle whose INDEX equals the cell
+    // index, as memory holds it at merge time (SPH-2D/sph_system.cu:1207)
+    auto cell_score_of = [&](uint32_t cell) -> float {
+        if (c.merge_rule != SPH_MERGE_WAVELET_CELL) return 0.f;
+        float eq, sq;
+        const uint32_t n_after = n + (split_on ? cnt->n_split * extra : 0u);
+        if (cell < n) {
+            const uint32_t sl = w.inv[cell];
+            eq = w.senergy[sl]; sq = w.ssurf[sl];
+        } else if (cell < n_after) {
+            const uint32_t sl = w.inv[w.split_list[(cell - n) / extra]];
+            eq = w.senergy[sl]; sq = w.ssurf[sl];
+        } else if (cell < cap) {
+            eq = st.energy[cell]; sq = st.surface[cell];
+        } else {
+            eq = 0.f; sq = 0.f;   // beyond the allocation: treated as zeroed memory
         }
-        uint32_t count = 0;
-        for (uint32_t base = b; base < e; base += 32) {
-            const uint32_t t = base + lane;
-            const int el = t < e ? merge_eligible<DIM>(c, w, t, split_on, ways, cell_score) : 0;
-            const uint32_t m = __ballot_sync(0xffffffffu, el);
-            const uint32_t r = count + __popc(m & ((1u << lane) - 1u));
-            if (el && r < kMergeListMax) list[wib][r] = t;
-            count += __popc(m);
+        return split_score(c, eq, sq);
+    };
+    // each warp takes 32 consecutive cells at a time; their members are one
+    // contiguous slot range, tested 32 slots at a time
+    for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + wib) * 32u; base < ncells; base += warps_total * 32u) {
+        const uint32_t cend = min(base + 32u, ncells);
+        const uint32_t sb = w.cell_off[base], se = w.cell_off[cend];
+        // every eligible member is listed with its cell and its rank among
+        // the cell's eligible members (cells are contiguous in slot order; the
+        // count of the chunk's last cell carries into the next chunk)
+        uint32_t len = 0, carry_cell = kEmpty, carry_cnt = 0;
+        for (uint32_t t0 = sb; t0 < se; t0 += 32) {
+            const uint32_t t = t0 + lane;
+            const bool in = t < se;
+            const uint32_t cell = in ? w.skey[t] : kEmpty;
+            const int el = in ? merge_eligible<DIM>(c, w, t, split_on, ways, cell_score_of(cell)) : 0;
+            const unsigned same = __match_any_sync(full, cell);
+            const unsigned eb = __ballot_sync(full, el);
+            const uint32_t rank = __popc(eb & same & lt) + (cell == carry_cell ? carry_cnt : 0u);
+            const uint32_t pos = len + __popc(eb & lt);
+            if (el && pos < (uint32_t)kMergeListMax) {
+                list[wib][pos] = t;
+                lcell[wib][pos] = cell;
+                lrank[wib][pos] = (uint8_t)min(rank, 255u);   // a rank inside the list is below its length
+            }
+            len += __popc(eb);
+            const int last = __popc(__ballot_sync(full, in)) - 1;
+            const uint32_t lc = __shfl_sync(full, cell, last);
+            const unsigned lsame = __shfl_sync(full, same, last);
+            carry_cnt = (lc == carry_cell ? carry_cnt : 0u) + __popc(eb & lsame);
+            carry_cell = lc;
         }
         __syncwarp();
-        const uint32_t groups = count / ways;
-        if (count <= (uint32_t)kMergeListMax) {
-            for (uint32_t g = lane; g < groups; g += 32)
-                merge_group<DIM>(c, w, &list[wib][g * ways], ways, split_on, hs2);
-        } else if (lane == 0) {
-            // more eligible members than the per-warp list holds: walk the
-            // cell serially with the same group arithmetic
-            uint32_t grp[4], got = 0, done = 0;
-            for (uint32_t t = b; t < e && done < groups; ++t) {
-                if (!merge_eligible<DIM>(c, w, t, split_on, ways, cell_score)) continue;
-                grp[got++] = t;
-                if (got == ways) {
-                    merge_group<DIM>(c, w, grp, ways, split_on, hs2);
-                    got = 0;
-                    ++done;
+        if (len <= (uint32_t)kMergeListMax) {
+            // a group = `ways` consecutive eligible members of one cell, from
+            // rank 0 on; its first member is the survivor
+            for (uint32_t k = lane; k < len; k += 32)
+                if (lrank[wib][k] % ways == 0 && k + ways - 1 < len && lcell[wib][k + ways - 1] == lcell[wib][k])
+                    merge_group<DIM>(c, w, &list[wib][k], ways, split_on, hs2);
+            __syncwarp();
+            continue;
+        }
+        // more eligible members than the list holds: the cells one at a time
+        const uint32_t mine = base + lane;
+        const uint32_t members = mine < cend ? w.cell_off[mine + 1] - w.cell_off[mine] : 0u;
+        uint32_t todo = __ballot_sync(full, members >= ways);
+        while (todo) {
+            const uint32_t cell = base + (__ffs(todo) - 1);
+            todo &= todo - 1;
+            const uint32_t b = w.cell_off[cell], e = w.cell_off[cell + 1];
+            const float cell_score = cell_score_of(cell);
+            uint32_t count = 0;
+            for (uint32_t t0 = b; t0 < e; t0 += 32) {
+                const uint32_t t = t0 + lane;
+                const int el = t < e ? merge_eligible<DIM>(c, w, t, split_on, ways, cell_score) : 0;
+                const unsigned m = __ballot_sync(full, el);
+                const uint32_t r = count + __popc(m & lt);
+                if (el && r < (uint32_t)kMergeListMax) list[wib][r] = t;
+                count += __popc(m);
+            }
+            __syncwarp();
+            const uint32_t groups = count / ways;
+            if (count <= (uint32_t)kMergeListMax) {
+                for (uint32_t g = lane; g < groups; g += 32)
+                    merge_group<DIM>(c, w, &list[wib][g * ways], ways, split_on, hs2);
+            } else if (lane == 0) {
+                // more eligible members than the list holds: walk the cell
+                // serially with the same group arithmetic
+                uint32_t grp[4], got = 0, done = 0;
+                for (uint32_t t = b; t < e && done < groups; ++t) {
+                    if (!merge_eligible<DIM>(c, w, t, split_on, ways, cell_score)) continue;
+                    grp[got++] = t;
+                    if (got == ways) {
+                        merge_group<DIM>(c, w, grp, ways, split_on, hs2);
+                        got = 0;
+                        ++done;
+                    }
                 }
             }
-        }
-        __syncwarp();
+            __syncwarp();
         }
     }
 }
