@@ -381,6 +381,7 @@ int sph_create(const sph_config *cfg, sph_handle **out)
     // stencil themselves
     w.nlist = nullptr;
     w.ncnt = nullptr;
+    w.nl_stride = (uint32_t)cap;
     if ((uint64_t)cap * kNbrListCap * sizeof(uint32_t) <= (12ull << 30)) {
         rc |= dalloc(h, &w.nlist, cap * kNbrListCap);
         rc |= dalloc(h, &w.ncnt, cap);
@@ -1180,7 +1181,8 @@ int sph_autotune(sph_handle *h, uint32_t reps, sph_tuning *out)
     static const uint32_t kBpsm[5] = {2, 4, 8, 16, 32};
     for (int st = 0; st < SPH_TUNE_STAGES && !rc; ++st) {
         if (st == SPH_TUNE_MERGE && !h->cfg.use_merge) continue;
-        uint32_t best_bs = h->tune_bs[st], best_bp = h->tune_bpsm[st], best_cap = h->tune_minb[st];
+        const uint32_t inc_bs = h->tune_bs[st], inc_bp = h->tune_bpsm[st], inc_cap = h->tune_minb[st];
+        uint32_t best_bs = inc_bs, best_bp = inc_bp, best_cap = inc_cap;
         if ((rc = trial())) break;
         float best = stage_ms[st];
         for (uint32_t cap = 0; cap <= 1 && !rc; ++cap)
@@ -1199,6 +1201,23 @@ int sph_autotune(sph_handle *h, uint32_t reps, sph_tuning *out)
                         best_cap = cap;
                     }
                 }
+        // a change must win a second, fresh comparison with the shape it replaces
+        if (!rc && (best_bs != inc_bs || best_bp != inc_bp || best_cap != inc_cap)) {
+            h->tune_bs[st] = best_bs;
+            h->tune_bpsm[st] = best_bp;
+            h->tune_minb[st] = best_cap;
+            if (!(rc = trial())) {
+                const float t_new = stage_ms[st];
+                h->tune_bs[st] = inc_bs;
+                h->tune_bpsm[st] = inc_bp;
+                h->tune_minb[st] = inc_cap;
+                if (!(rc = trial()) && !(t_new < stage_ms[st] * 0.98f)) {
+                    best_bs = inc_bs;
+                    best_bp = inc_bp;
+                    best_cap = inc_cap;
+                }
+            }
+        }
         h->tune_bs[st] = best_bs;
         h->tune_bpsm[st] = best_bp;
         h->tune_minb[st] = best_cap;

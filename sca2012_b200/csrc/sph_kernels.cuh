@@ -71,7 +71,8 @@ struct WorkPtrs {
     uint32_t *wall;                      // taped steps only: wall contacts per slot
     float4 *spos_lo, *spos_lo_n;         // low position parts per slot (compensated positions)
     uint32_t pos_comp;                   // the config's compensated_positions
-    uint32_t *nlist, *ncnt;              // neighbour candidates: nlist[slot * kNbrListCap + k], by the density pass
+    uint32_t *nlist, *ncnt;              // neighbour candidates (layout: nl_at), by the density pass
+    uint32_t nl_stride;                  // slots per list chunk row (the capacity)
 };
 
 // Neighbour candidates the density pass records per particle: every stencil
@@ -89,6 +90,14 @@ struct WorkPtrs {
 // Either way the sums are those of the walk, bit for bit.
 constexpr uint32_t kNbrListCap = 128;
 constexpr float kNbrListMargin = 0.05f;
+
+// Entry k of slot s's list.  Entries come in chunks of four (one 16-byte
+// load); chunk j of every slot is one row, so the chunk-j loads of a warp's
+// 32 consecutive slots read 512 contiguous bytes.
+__device__ __forceinline__ size_t nl_at(const WorkPtrs &w, uint32_t s, uint32_t k)
+{
+    return (size_t)(k >> 2) * ((size_t)w.nl_stride * 4u) + (size_t)s * 4u + (k & 3u);
+}
 
 __device__ __forceinline__ float energy_list_r2(const sph_config &c)
 {
@@ -377,7 +386,6 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restri
         const bool rec = w.nlist != nullptr;
         const float re2 = energy_list_r2(c);
         const float prune = rec ? fmaxf(re2, h2) : h2;
-        uint32_t *mine = rec ? w.nlist + (size_t)s * kNbrListCap : nullptr;   // a particle's entries share sectors
         // single pass: the kernel sum is cheap enough to run predicated
         // (:394-417, j != i with skip <= r^2 < h_i^2)
         auto add = [&](uint32_t t, float4 pj) {
@@ -390,7 +398,7 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restri
                     ++nb;
                 }
                 if (rec && r2 < re2) {
-                    if (nl < kNbrListCap) mine[nl] = t;
+                    if (nl < kNbrListCap) w.nlist[nl_at(w, s, nl)] = t;
                     ++nl;
                 }
             }
@@ -507,12 +515,11 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
             // the density pass's candidates, filtered by the walk's test: same
             // neighbours, same order as the walk
             const uint32_t m = __reduce_max_sync(full, nf);
-            const uint32_t *mine = w.nlist + (size_t)s * kNbrListCap;
             uint32_t kk = 0;
             // four entries per 16-byte load, their neighbours' loads issued
             // before the math (entries past nf are replaced by the particle itself)
             for (; kk + 4 <= m; kk += 4) {
-                const uint4 t4 = *reinterpret_cast<const uint4 *>(mine + kk);
+                const uint4 t4 = *reinterpret_cast<const uint4 *>(w.nlist + nl_at(w, s, kk));
                 const uint32_t tt[4] = {kk < nf ? t4.x : s, kk + 1 < nf ? t4.y : s, kk + 2 < nf ? t4.z : s,
                                         kk + 3 < nf ? t4.w : s};
                 float4 pj[4], aj[4], ej[4];
@@ -528,7 +535,7 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
             }
             for (; kk < m; ++kk)
                 if (kk < nf) {
-                    const uint32_t t = mine[kk];
+                    const uint32_t t = w.nlist[nl_at(w, s, kk)];
                     const float4 pj = w.spos[t];
                     if (accept(t, pj)) pair_with(pj, w.saux[t], w.sev[t]);
                 }
@@ -724,11 +731,11 @@ __global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counter
         }
         const uint32_t m = __reduce_max_sync(0xffffffffu, ne);
         if (m) {
-            const uint32_t *mine = w.nlist + (size_t)s * kNbrListCap;
             // four entries per 16-byte load, their neighbours fetched before the
             // math (entries past ne are replaced by the particle itself)
             for (uint32_t kk = 0; kk < m; kk += 4) {
-                const uint4 t4 = kk < ne ? *reinterpret_cast<const uint4 *>(mine + kk) : make_uint4(s, s, s, s);
+                const uint4 t4 = kk < ne ? *reinterpret_cast<const uint4 *>(w.nlist + nl_at(w, s, kk))
+                                         : make_uint4(s, s, s, s);
                 const uint32_t tt[4] = {kk < ne ? t4.x : s, kk + 1 < ne ? t4.y : s, kk + 2 < ne ? t4.z : s,
                                         kk + 3 < ne ? t4.w : s};
                 NbrPV g[4];
