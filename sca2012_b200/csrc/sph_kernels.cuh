@@ -190,31 +190,6 @@ __device__ __forceinline__ int row_range(const sph_config &c, const uint32_t *__
     return 1;
 }
 
-// As row_range, for FRESH cell lists (every member lies inside its cell):
-// drops the row when the slab it spans in y/z is farther from p than the
-// cut-off, and the row's end cells when they are.  A cell is dropped only if
-// its distance exceeds sqrt(cut2 * 1.001), far above the FP32 rounding of
-// the positions, so every pair the exact r^2 test accepts stays in range.
-template <int DIM>
-__device__ __forceinline__ int row_range_pruned(const sph_config &c, const uint32_t *__restrict__ off, uint3 q,
-                                                float4 p, float cut2, int dy, int dz, uint32_t &b, uint32_t &e)
-{
-    int y = (int)q.y + dy, z = (int)q.z + dz;
-    if (y < 0 || y >= (int)c.ncell[1]) return 0;
-    if (DIM == 3 && (z < 0 || z >= (int)c.ncell[2])) return 0;
-    const float cs = c.cell_size, lim = cut2 * 1.001f;
-    const float ey = dy < 0 ? p.y - (float)q.y * cs : (dy > 0 ? (float)(q.y + 1) * cs - p.y : 0.0f);
-    const float ez = DIM == 3 ? (dz < 0 ? p.z - (float)q.z * cs : (dz > 0 ? (float)(q.z + 1) * cs - p.z : 0.0f)) : 0.0f;
-    const float base = fmaxf(ey, 0.0f) * fmaxf(ey, 0.0f) + fmaxf(ez, 0.0f) * fmaxf(ez, 0.0f);
-    if (!(base < lim)) return 0;
-    const float ex0 = fmaxf(p.x - (float)q.x * cs, 0.0f), ex1 = fmaxf((float)(q.x + 1) * cs - p.x, 0.0f);
-    const uint32_t x0 = (q.x > 0 && ex0 * ex0 + base < lim) ? q.x - 1 : q.x;
-    const uint32_t x1 = (q.x + 1 < c.ncell[0] && ex1 * ex1 + base < lim) ? q.x + 1 : q.x;
-    b = __ldg(off + key_of(c, x0, (uint32_t)y, (uint32_t)z));
-    e = __ldg(off + key_of(c, x1, (uint32_t)y, (uint32_t)z) + 1);
-    return 1;
-}
-
 // ------------------------------------------------------------ 1. hash
 template <int DIM, int BS = kThreads>
 __global__ void __launch_bounds__(BS) k_hash(sph_config c, const Counters *__restrict__ cnt,
@@ -385,7 +360,6 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restri
         // (r^2 < (1 + margin)^2 h_max^2), in the order their walks find them
         const bool rec = w.nlist != nullptr;
         const float re2 = energy_list_r2(c);
-        const float prune = rec ? fmaxf(re2, h2) : h2;
         // single pass: the kernel sum is cheap enough to run predicated
         // (:394-417, j != i with skip <= r^2 < h_i^2)
         auto add = [&](uint32_t t, float4 pj) {
@@ -408,7 +382,7 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restri
 #pragma unroll 1
             for (int dy = -1; dy <= 1; ++dy) {
                 uint32_t b, e;
-                if (!row_range_pruned<DIM>(c, w.cell_off, q, pi, prune, dy, dz, b, e)) continue;
+                if (!row_range<DIM>(c, w.cell_off, q, dy, dz, b, e)) continue;
                 uint32_t t = b;
                 for (; t + 4 <= e; t += 4) {
                     const float4 p0 = w.spos[t], p1 = w.spos[t + 1], p2 = w.spos[t + 2], p3 = w.spos[t + 3];
