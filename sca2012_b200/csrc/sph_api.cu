@@ -376,6 +376,7 @@ int sph_create(const sph_config *cfg, sph_handle **out)
     rc |= dalloc(h, &w.snbr, cap); rc |= dalloc(h, &w.sinter, cap);
     rc |= dalloc(h, &w.stv, cap); rc |= dalloc(h, &w.sscene, cap);
     rc |= dalloc(h, &w.spos_lo, cap); rc |= dalloc(h, &w.spos_lo_n, cap);
+    rc |= dalloc(h, &w.fnb_a, cap); rc |= dalloc(h, &w.fnb_b, cap);
     // neighbour candidate lists (512 B per particle of capacity); without
     // them (very large capacities) the force and energy kernels walk the
     // stencil themselves

@@ -73,6 +73,8 @@ struct WorkPtrs {
     uint32_t pos_comp;                   // the config's compensated_positions
     uint32_t *nlist, *ncnt;              // neighbour candidates (layout: nl_at), by the density pass
     uint32_t nl_stride;                  // slots per list chunk row (the capacity)
+    float4 *fnb_a, *fnb_b;               // a force neighbour in two loads: (x, y, z, p/rho^2) and
+                                         // (m/rho with the sign bit set for level 2, ev.xyz), by the density pass
 };
 
 // Neighbour candidates the density pass records per particle: every stencil
@@ -397,7 +399,11 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restri
         float r = rho / c.rest_density;
         const float gas = w.nscenes ? w.scene_tab[2 * min(w.sscene[s], w.nscenes - 1u) + 1].w : c.gas_constant;
         float p = (r * r * r - 1.0f) * gas;
-        w.saux[s] = make_float4(rho, p, p / (rho * rho), c.mass[li] / rho);
+        const float pr2 = p / (rho * rho), mr = c.mass[li] / rho;
+        w.saux[s] = make_float4(rho, p, pr2, mr);
+        const float4 evs = w.sev[s];
+        w.fnb_a[s] = make_float4(pi.x, pi.y, pi.z, pr2);
+        w.fnb_b[s] = make_float4(li ? -mr : mr, evs.x, evs.y, evs.z);
         w.snbr[s] = nb;
         if (rec) w.ncnt[s] = nl;
     }
@@ -456,10 +462,12 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
             return t != s && r2 < cut && !(r2 < close);
         };
         // pressure, viscosity and colour-field terms of one neighbour
-        auto pair_with = [&](const float4 pj, const float4 aj, const float4 evj) {
+        // (a, b: the neighbour's two records)
+        auto pair_ab = [&](const float4 a, const float4 b) {
             float rx, ry, rz;
-            const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
-            const int lj = lv(pj.w);
+            const float r2 = r2_of<DIM>(pi, a, rx, ry, rz);
+            const int lj = signbit(b.x) ? 1 : 0;
+            const float mrj = fabsf(b.x);   // m_j/rho_j
             const float r = __fsqrt_rn(r2);
             float ipk = 0.f, ivk = 0.f, jpk = 0.f, jvk = 0.f;
             const float ikr = __fsub_rn(hi, r);
@@ -467,22 +475,28 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
                 ipk = ispk * ikr * ikr;
                 ivk = ivis * ikr;
                 const float x = hi2 - r2;
-                const float tg = igrad * aj.w * x * x;   // -grad_poly6 * m_j/rho_j * (h^2-r^2)^2
+                const float tg = igrad * mrj * x * x;   // -grad_poly6 * m_j/rho_j * (h^2-r^2)^2
                 gx += tg * rx; gy += tg * ry; gz += tg * rz;
-                lap += ilap * aj.w * x * (r2 - c.lapc_three_quarters * x);
+                lap += ilap * mrj * x * (r2 - c.lapc_three_quarters * x);
             }
             const float jkr = __fsub_rn(c.kernel[lj], r);
             if (jkr > 0.0f) {
                 jpk = (lj ? jspk1 : jspk0) * jkr * jkr;
                 jvk = (lj ? jvis1 : jvis0) * jkr;
             }
-            const float tp = (lj ? mimj1 : mimj0) * (ai.z + aj.z) * (ipk + jpk) * 0.5f / r;
-            const float tv = (ai.w * aj.w) * visc * (ivk + jvk) * 0.5f;
-            fx += -rx * tp + (evj.x - evi.x) * tv;
-            fy += -ry * tp + (evj.y - evi.y) * tv;
-            if (DIM == 3) fz += -rz * tp + (evj.z - evi.z) * tv;
+            const float tp = (lj ? mimj1 : mimj0) * (ai.z + a.w) * (ipk + jpk) * 0.5f / r;
+            const float tv = (ai.w * mrj) * visc * (ivk + jvk) * 0.5f;
+            fx += -rx * tp + (b.y - evi.x) * tv;
+            fy += -ry * tp + (b.z - evi.y) * tv;
+            if (DIM == 3) fz += -rz * tp + (b.w - evi.z) * tv;
         };
-        auto pair = [&](uint32_t t) { pair_with(w.spos[t], w.saux[t], w.sev[t]); };
+        auto accept_ab = [&](uint32_t t, const float4 &a, const float4 &b) {
+            float rx, ry, rz;
+            const float r2 = r2_of<DIM>(pi, a, rx, ry, rz);
+            const float cut = signbit(b.x) ? cut1 : cut0;
+            return t != s && r2 < cut && !(r2 < close);
+        };
+        auto pair = [&](uint32_t t) { pair_ab(w.fnb_a[t], w.fnb_b[t]); };
         const unsigned full = 0xffffffffu;
         const uint32_t nf = valid && w.nlist ? w.ncnt[s] : 0u;
         if (__all_sync(full, w.nlist != nullptr && nf <= kNbrListCap)) {
@@ -496,22 +510,21 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
                 const uint4 t4 = *reinterpret_cast<const uint4 *>(w.nlist + nl_at(w, s, kk));
                 const uint32_t tt[4] = {kk < nf ? t4.x : s, kk + 1 < nf ? t4.y : s, kk + 2 < nf ? t4.z : s,
                                         kk + 3 < nf ? t4.w : s};
-                float4 pj[4], aj[4], ej[4];
+                float4 na[4], nb[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
-                    pj[u] = w.spos[tt[u]];
-                    aj[u] = w.saux[tt[u]];
-                    ej[u] = w.sev[tt[u]];
+                    na[u] = w.fnb_a[tt[u]];
+                    nb[u] = w.fnb_b[tt[u]];
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
-                    if (kk + u < nf && accept(tt[u], pj[u])) pair_with(pj[u], aj[u], ej[u]);
+                    if (kk + u < nf && accept_ab(tt[u], na[u], nb[u])) pair_ab(na[u], nb[u]);
             }
             for (; kk < m; ++kk)
                 if (kk < nf) {
                     const uint32_t t = w.nlist[nl_at(w, s, kk)];
-                    const float4 pj = w.spos[t];
-                    if (accept(t, pj)) pair_with(pj, w.saux[t], w.sev[t]);
+                    const float4 a = w.fnb_a[t], b = w.fnb_b[t];
+                    if (accept_ab(t, a, b)) pair_ab(a, b);
                 }
         } else {
             warp_pairs<DIM>(c, w.cell_off, w.spos, valid, q, smem[wib], accept, pair);
