@@ -353,7 +353,8 @@ def run_ours(args, rank, world, local_rank):
                          "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_particle": STAGE_BYTES.get(top),
                          "launch_ms": stage_avg[top], "peak_source": peak_src,
-                         "note": "neighbour loops are FP32-issue bound: the HBM fraction is low by design",
+                         "note": ("neighbour loops are bound by FP32 issue (density) and dependent-load latency "
+                                  "(force, energy): the HBM fraction is low by design"),
                          "neighbour_loops": {"stages": ["density", "force_integrate", "energy_split"],
                                              "bytes_per_particle": 128, "ms": nl_ms, "achieved": nl_gbs,
                                              "frac": nl_gbs / peak if nl_gbs else None}},
