@@ -202,7 +202,14 @@ __global__ void __launch_bounds__(BS) k_hash(sph_config c, const Counters *__res
         uint3 q = cell_of<DIM>(c, st.pos[i]);
         uint32_t k = key_of(c, q.x, q.y, q.z);
         w.key[i] = k;
-        w.slot[i] = atomicAdd(w.cell_count + k, 1u);
+        // one atomic per group of lanes in the same cell (consecutive particles
+        // often share one); any distinct slots do, k_reorder restores the order
+        const unsigned grp = __match_any_sync(__activemask(), k);
+        const int lead = __ffs(grp) - 1, lane = threadIdx.x & 31;
+        uint32_t first = 0;
+        if (lane == lead) first = atomicAdd(w.cell_count + k, (uint32_t)__popc(grp));
+        first = __shfl_sync(grp, first, lead);
+        w.slot[i] = first + __popc(grp & ((1u << lane) - 1u));
     }
 }
 
@@ -362,6 +369,8 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restri
         // (r^2 < (1 + margin)^2 h_max^2), in the order their walks find them
         const bool rec = w.nlist != nullptr;
         const float re2 = energy_list_r2(c);
+        // (m_j * poly6) once per level: the same product the sum takes first
+        const float mp0 = m0 * poly6, mp1 = m1 * poly6;
         // single pass: the kernel sum is cheap enough to run predicated
         // (:394-417, j != i with skip <= r^2 < h_i^2)
         auto add = [&](uint32_t t, float4 pj) {
@@ -370,7 +379,7 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restri
             if (t != s) {
                 if (!(r2 < skip) && r2 < h2) {
                     const float x = h2 - r2;
-                    rho += (pj.w == 1.0f ? m0 : m1) * poly6 * (x * x * x);
+                    rho += (pj.w == 1.0f ? mp0 : mp1) * (x * x * x);
                     ++nb;
                 }
                 if (rec && r2 < re2) {
