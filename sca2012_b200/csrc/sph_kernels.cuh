@@ -373,20 +373,33 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restri
         const float mp0 = m0 * poly6, mp1 = m1 * poly6;
         // single pass: the kernel sum is cheap enough to run predicated
         // (:394-417, j != i with skip <= r^2 < h_i^2)
-        auto add = [&](uint32_t t, float4 pj) {
+        // list entry k at lbase[(k >> 2) * row4 + (k & 3)] (nl_at; the offset
+        // fits 32 bits under the lists' 12 GB allocation limit)
+        uint32_t *const lbase = rec ? w.nlist + (size_t)s * 4u : nullptr;
+        const uint32_t row4 = w.nl_stride * 4u;
+        auto add = [&](uint32_t t, float4 pj) {   // t != s (the walk skips s)
             float dx, dyy, dzz;
             const float r2 = r2_of<DIM>(pj, pi, dx, dyy, dzz);
-            if (t != s) {
-                if (!(r2 < skip) && r2 < h2) {
-                    const float x = h2 - r2;
-                    rho += (pj.w == 1.0f ? mp0 : mp1) * (x * x * x);
-                    ++nb;
-                }
-                if (rec && r2 < re2) {
-                    if (nl < kNbrListCap) w.nlist[nl_at(w, s, nl)] = t;
-                    ++nl;
-                }
+            if (!(r2 < skip) && r2 < h2) {
+                const float x = h2 - r2;
+                rho += (pj.w == 1.0f ? mp0 : mp1) * (x * x * x);
+                ++nb;
             }
+            if (rec && r2 < re2) {
+                if (nl < kNbrListCap) lbase[(nl >> 2) * row4 + (nl & 3u)] = t;
+                ++nl;
+            }
+        };
+        auto range = [&](uint32_t b, uint32_t e) {
+            uint32_t t = b;
+            for (; t + 4 <= e; t += 4) {
+                const float4 p0 = w.spos[t], p1 = w.spos[t + 1], p2 = w.spos[t + 2], p3 = w.spos[t + 3];
+                add(t, p0);
+                add(t + 1, p1);
+                add(t + 2, p2);
+                add(t + 3, p3);
+            }
+            for (; t < e; ++t) add(t, w.spos[t]);
         };
 #pragma unroll 1
         for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
@@ -394,15 +407,12 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restri
             for (int dy = -1; dy <= 1; ++dy) {
                 uint32_t b, e;
                 if (!row_range<DIM>(c, w.cell_off, q, dy, dz, b, e)) continue;
-                uint32_t t = b;
-                for (; t + 4 <= e; t += 4) {
-                    const float4 p0 = w.spos[t], p1 = w.spos[t + 1], p2 = w.spos[t + 2], p3 = w.spos[t + 3];
-                    add(t, p0);
-                    add(t + 1, p1);
-                    add(t + 2, p2);
-                    add(t + 3, p3);
+                if (dy == 0 && dz == 0) {   // the particle's own row: around its slot
+                    range(b, s);
+                    range(s + 1u, e);
+                } else {
+                    range(b, e);
                 }
-                for (; t < e; ++t) add(t, w.spos[t]);
             }
         rho += c.mass[li] * poly6 * c.kernel6[li];   // self term
         float r = rho / c.rest_density;
