@@ -509,11 +509,12 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
             fy += -ry * tp + (b.z - evi.y) * tv;
             if (DIM == 3) fz += -rz * tp + (b.w - evi.z) * tv;
         };
-        auto accept_ab = [&](uint32_t t, const float4 &a, const float4 &b) {
+        // the walk's test for a list entry (a list never holds the particle itself)
+        auto accept_ab = [&](const float4 &a, const float4 &b) {
             float rx, ry, rz;
             const float r2 = r2_of<DIM>(pi, a, rx, ry, rz);
             const float cut = signbit(b.x) ? cut1 : cut0;
-            return t != s && r2 < cut && !(r2 < close);
+            return r2 < cut && !(r2 < close);
         };
         auto pair = [&](uint32_t t) { pair_ab(w.fnb_a[t], w.fnb_b[t]); };
         const unsigned full = 0xffffffffu;
@@ -537,13 +538,13 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
-                    if (kk + u < nf && accept_ab(tt[u], na[u], nb[u])) pair_ab(na[u], nb[u]);
+                    if (kk + u < nf && accept_ab(na[u], nb[u])) pair_ab(na[u], nb[u]);
             }
             for (; kk < m; ++kk)
                 if (kk < nf) {
                     const uint32_t t = w.nlist[nl_at(w, s, kk)];
                     const float4 a = w.fnb_a[t], b = w.fnb_b[t];
-                    if (accept_ab(t, a, b)) pair_ab(a, b);
+                    if (accept_ab(a, b)) pair_ab(a, b);
                 }
         } else {
             warp_pairs<DIM>(c, w.cell_off, w.spos, valid, q, smem[wib], accept, pair);
