@@ -93,6 +93,12 @@ struct WorkPtrs {
 constexpr uint32_t kNbrListCap = 128;
 constexpr float kNbrListMargin = 0.05f;
 
+// Pulls a line into L2 ahead of its use (no register, no result).
+__device__ __forceinline__ void prefetch_l2(const void *p)
+{
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // Entry k of slot s's list.  Entries come in chunks of four (one 16-byte
 // load); chunk j of every slot is one row, so the chunk-j loads of a warp's
 // 32 consecutive slots read 512 contiguous bytes.
@@ -527,6 +533,7 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
             // four entries per 16-byte load, their neighbours' loads issued
             // before the math (entries past nf are replaced by the particle itself)
             for (; kk + 4 <= m; kk += 4) {
+                if (kk + 8 < m) prefetch_l2(w.nlist + nl_at(w, s, kk + 8));   // two rounds ahead
                 const uint4 t4 = *reinterpret_cast<const uint4 *>(w.nlist + nl_at(w, s, kk));
                 const uint32_t tt[4] = {kk < nf ? t4.x : s, kk + 1 < nf ? t4.y : s, kk + 2 < nf ? t4.z : s,
                                         kk + 3 < nf ? t4.w : s};
@@ -741,6 +748,7 @@ __global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counter
             // four entries per 16-byte load, their neighbours fetched before the
             // math (entries past ne are replaced by the particle itself)
             for (uint32_t kk = 0; kk < m; kk += 4) {
+                if (kk + 8 < m) prefetch_l2(w.nlist + nl_at(w, s, kk + 8));   // two rounds ahead
                 const uint4 t4 = kk < ne ? *reinterpret_cast<const uint4 *>(w.nlist + nl_at(w, s, kk))
                                          : make_uint4(s, s, s, s);
                 const uint32_t tt[4] = {kk < ne ? t4.x : s, kk + 1 < ne ? t4.y : s, kk + 2 < ne ? t4.z : s,
