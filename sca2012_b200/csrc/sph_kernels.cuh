@@ -532,8 +532,9 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
             uint32_t kk = 0;
             // four entries per 16-byte load, their neighbours' loads issued
             // before the math (entries past nf are replaced by the particle itself)
+            if (4 < m) prefetch_l2(w.nlist + nl_at(w, s, 4));
             for (; kk + 4 <= m; kk += 4) {
-                if (kk + 8 < m) prefetch_l2(w.nlist + nl_at(w, s, kk + 8));   // two rounds ahead
+                if (kk + 8 < m) prefetch_l2(w.nlist + nl_at(w, s, kk + 8));   // 2 rounds ahead
                 const uint4 t4 = *reinterpret_cast<const uint4 *>(w.nlist + nl_at(w, s, kk));
                 const uint32_t tt[4] = {kk < nf ? t4.x : s, kk + 1 < nf ? t4.y : s, kk + 2 < nf ? t4.z : s,
                                         kk + 3 < nf ? t4.w : s};
@@ -747,8 +748,9 @@ __global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counter
         if (m) {
             // four entries per 16-byte load, their neighbours fetched before the
             // math (entries past ne are replaced by the particle itself)
+            if (4 < m) prefetch_l2(w.nlist + nl_at(w, s, 4));
             for (uint32_t kk = 0; kk < m; kk += 4) {
-                if (kk + 8 < m) prefetch_l2(w.nlist + nl_at(w, s, kk + 8));   // two rounds ahead
+                if (kk + 8 < m) prefetch_l2(w.nlist + nl_at(w, s, kk + 8));   // 2 rounds ahead
                 const uint4 t4 = kk < ne ? *reinterpret_cast<const uint4 *>(w.nlist + nl_at(w, s, kk))
                                          : make_uint4(s, s, s, s);
                 const uint32_t tt[4] = {kk < ne ? t4.x : s, kk + 1 < ne ? t4.y : s, kk + 2 < ne ? t4.z : s,
