@@ -163,10 +163,19 @@ __global__ void __launch_bounds__(kThreads) adj_integrate(sph_config c, StepCoun
 }
 
 // ---------------------------------------------------------------- force pairs
+// The pairs are found by the warp-lockstep stencil walk of the forward force
+// pass (warp_pairs): each lane adds its pairs in walk order, so the sums do
+// not depend on which particles share its warp.
 template <int DIM>
 __global__ void __launch_bounds__(kThreads) adj_force(sph_config c, StepCounts k, TapeStep t, WorkPtrs w, AdjPtrs a)
 {
-    for (uint32_t s = grid_stride_start(); s < k.n; s += grid_stride()) {
+    __shared__ WarpPairSmem smem[kThreads / 32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const uint32_t n = k.n;
+    for (uint32_t base = blockIdx.x * kThreads + wib * 32u; base < n; base += gridDim.x * kThreads) {
+        const uint32_t s_raw = base + lane;
+        const bool valid = s_raw < n;
+        const uint32_t s = valid ? s_raw : n - 1u;
         const float4 pi = t.spos[s], evi = t.sev[s], ai = t.saux[s], gfi = a.gf[s];
         const int li = lv(pi.w);
         const float hi = c.kernel[li], hi2 = c.kernel2[li], mi = c.mass[li];
@@ -183,49 +192,48 @@ __global__ void __launch_bounds__(kThreads) adj_force(sph_config c, StepCounts k
         const float cut0 = fmaxf(hi2, c.kernel2[0]), cut1 = fmaxf(hi2, c.kernel2[1]);
         float4 gx = make_float4(0.f, 0.f, 0.f, 0.f), ge = gx;
         float gA = 0.f, gV = 0.f, gmu = 0.f;
-#pragma unroll 1
-        for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
-#pragma unroll 1
-            for (int dy = -1; dy <= 1; ++dy) {
-                uint32_t b, e;
-                if (!row_range<DIM>(c, t.cell_off, q, dy, dz, b, e)) continue;
-                for (uint32_t j = b; j < e; ++j) {
-                    if (j == s) continue;
-                    const float4 pj = t.spos[j];
-                    float rx, ry, rz;
-                    const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
-                    const float cut = pj.w == 1.0f ? cut0 : cut1;
-                    if (!(r2 < cut) || r2 < c.close_r2) continue;
-                    const int lj = lv(pj.w);
-                    const float r = __fsqrt_rn(r2);
-                    const float ikr = __fsub_rn(hi, r), jkr = __fsub_rn(c.kernel[lj], r);
-                    float S = 0.f, dS = 0.f, T = 0.f, dT = 0.f;
-                    if (ikr > 0.0f) { S += ispk * ikr * ikr; dS -= 2.0f * ispk * ikr; T += ivis * ikr; dT -= ivis; }
-                    if (jkr > 0.0f) {
-                        const float jspk = c.kernel_h6_twice ? c.spiky[lj] / c.kernel6[lj] : c.spiky[lj];
-                        const float jvis = c.kernel_h6_twice ? c.visco[lj] / c.kernel6[lj] : c.visco[lj];
-                        S += jspk * jkr * jkr; dS -= 2.0f * jspk * jkr; T += jvis * jkr; dT -= jvis;
-                    }
-                    const float4 aj = t.saux[j], evj = t.sev[j], gfj = a.gf[j];
-                    const float mm = mi * c.mass[lj];
-                    const float Cp = mm * (ai.z + aj.z) * 0.5f;
-                    const float ir = 1.0f / r;
-                    const float tp = Cp * S * ir, dtp = Cp * (dS - S * ir) * ir;
-                    const float VV = ai.w * aj.w;
-                    const float tv = VV * visc * 0.5f * T, dtv = VV * visc * 0.5f * dT;
-                    const float4 D = sub3(gfi, gfj);
-                    const float4 rv = make_float4(rx, ry, rz, 0.f);
-                    const float4 dv = sub3(evj, evi);
-                    const float Dr = dot3(D, rv), Ddv = dot3(D, dv);
-                    const float coef = (Ddv * dtv - Dr * dtp) * ir;
-                    axpy3(gx, -tp, D);
-                    axpy3(gx, coef, rv);
-                    axpy3(ge, -tv, D);
-                    gA -= Dr * mm * 0.5f * S * ir;
-                    gV += Ddv * aj.w * visc * 0.5f * T;
-                    gmu += 0.25f * Ddv * VV * T;     // each unordered pair is visited from both ends
-                }
+        // the forward pass's pairs: j != i, r^2 < max(h_i^2, h_j^2), r^2 >= close_r2
+        auto accept = [&](uint32_t j, const float4 &pj) {
+            float rx, ry, rz;
+            const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
+            const float cut = pj.w == 1.0f ? cut0 : cut1;
+            return j != s && r2 < cut && !(r2 < c.close_r2);
+        };
+        auto pair = [&](uint32_t j) {
+            const float4 pj = t.spos[j];
+            float rx, ry, rz;
+            const float r2 = r2_of<DIM>(pi, pj, rx, ry, rz);
+            const int lj = lv(pj.w);
+            const float r = __fsqrt_rn(r2);
+            const float ikr = __fsub_rn(hi, r), jkr = __fsub_rn(c.kernel[lj], r);
+            float S = 0.f, dS = 0.f, T = 0.f, dT = 0.f;
+            if (ikr > 0.0f) { S += ispk * ikr * ikr; dS -= 2.0f * ispk * ikr; T += ivis * ikr; dT -= ivis; }
+            if (jkr > 0.0f) {
+                const float jspk = c.kernel_h6_twice ? c.spiky[lj] / c.kernel6[lj] : c.spiky[lj];
+                const float jvis = c.kernel_h6_twice ? c.visco[lj] / c.kernel6[lj] : c.visco[lj];
+                S += jspk * jkr * jkr; dS -= 2.0f * jspk * jkr; T += jvis * jkr; dT -= jvis;
             }
+            const float4 aj = t.saux[j], evj = t.sev[j], gfj = a.gf[j];
+            const float mm = mi * c.mass[lj];
+            const float Cp = mm * (ai.z + aj.z) * 0.5f;
+            const float ir = 1.0f / r;
+            const float tp = Cp * S * ir, dtp = Cp * (dS - S * ir) * ir;
+            const float VV = ai.w * aj.w;
+            const float tv = VV * visc * 0.5f * T, dtv = VV * visc * 0.5f * dT;
+            const float4 D = sub3(gfi, gfj);
+            const float4 rv = make_float4(rx, ry, rz, 0.f);
+            const float4 dv = sub3(evj, evi);
+            const float Dr = dot3(D, rv), Ddv = dot3(D, dv);
+            const float coef = (Ddv * dtv - Dr * dtp) * ir;
+            axpy3(gx, -tp, D);
+            axpy3(gx, coef, rv);
+            axpy3(ge, -tv, D);
+            gA -= Dr * mm * 0.5f * S * ir;
+            gV += Ddv * aj.w * visc * 0.5f * T;
+            gmu += 0.25f * Ddv * VV * T;     // each unordered pair is visited from both ends
+        };
+        warp_pairs<DIM>(c, t.cell_off, t.spos, valid, q, smem[wib], accept, pair);
+        if (!valid) continue;
         // p = gas ((rho/rho0)^3 - 1); A = p / rho^2; V = m / rho
         const float rho = ai.x, p = ai.y;
         const float rr = rho / c.rest_density;
@@ -257,31 +265,47 @@ __global__ void __launch_bounds__(kThreads) adj_density(sph_config c, StepCounts
         q.y = (key / c.ncell[0]) % c.ncell[1];
         q.z = DIM == 3 ? key / (c.ncell[0] * c.ncell[1]) : 0u;
         float4 gx = a.gxd[s];
+        auto visit = [&](uint32_t j, float4 pj) {   // j != s
+            float dx, dy_, dz_;
+            const float r2 = r2_of<DIM>(pj, pi, dx, dy_, dz_);   // d = x_j - x_i
+            if (r2 < skip) return;
+            const int lj = lv(pj.w);
+            float acc = 0.0f;
+            if (r2 < h2) {          // term of rho_i
+                const float x = h2 - r2;
+                acc += gri * c.mass[lj] * w6 * x * x;
+            }
+            const float hj2 = c.kernel2[lj];
+            if (r2 < hj2) {         // term of rho_j
+                const float x = hj2 - r2;
+                acc += a.grho[j] * mi * c.poly6[lj] * x * x;
+            }
+            // d/dx_i (h^2 - r^2)^3 = -6 (h^2 - r^2)^2 (x_i - x_j) = +6 (...)^2 d
+            gx.x += 6.0f * acc * dx; gx.y += 6.0f * acc * dy_; gx.z += 6.0f * acc * dz_;
+        };
+        // slot order, four candidates' loads in flight; the own row around s
+        auto range = [&](uint32_t b, uint32_t e) {
+            uint32_t j = b;
+            for (; j + 4 <= e; j += 4) {
+                const float4 p0 = t.spos[j], p1 = t.spos[j + 1], p2 = t.spos[j + 2], p3 = t.spos[j + 3];
+                visit(j, p0);
+                visit(j + 1, p1);
+                visit(j + 2, p2);
+                visit(j + 3, p3);
+            }
+            for (; j < e; ++j) visit(j, t.spos[j]);
+        };
 #pragma unroll 1
         for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
 #pragma unroll 1
             for (int dy = -1; dy <= 1; ++dy) {
                 uint32_t b, e;
                 if (!row_range<DIM>(c, t.cell_off, q, dy, dz, b, e)) continue;
-                for (uint32_t j = b; j < e; ++j) {
-                    if (j == s) continue;
-                    const float4 pj = t.spos[j];
-                    float dx, dy_, dz_;
-                    const float r2 = r2_of<DIM>(pj, pi, dx, dy_, dz_);   // d = x_j - x_i
-                    if (r2 < skip) continue;
-                    const int lj = lv(pj.w);
-                    float acc = 0.0f;
-                    if (r2 < h2) {          // term of rho_i
-                        const float x = h2 - r2;
-                        acc += gri * c.mass[lj] * w6 * x * x;
-                    }
-                    const float hj2 = c.kernel2[lj];
-                    if (r2 < hj2) {         // term of rho_j
-                        const float x = hj2 - r2;
-                        acc += a.grho[j] * mi * c.poly6[lj] * x * x;
-                    }
-                    // d/dx_i (h^2 - r^2)^3 = -6 (h^2 - r^2)^2 (x_i - x_j) = +6 (...)^2 d
-                    gx.x += 6.0f * acc * dx; gx.y += 6.0f * acc * dy_; gx.z += 6.0f * acc * dz_;
+                if (dy == 0 && dz == 0) {
+                    range(b, s);
+                    range(s + 1u, e);
+                } else {
+                    range(b, e);
                 }
             }
         const uint32_t i = t.sidx[s];
