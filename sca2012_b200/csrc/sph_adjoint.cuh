@@ -163,9 +163,63 @@ __global__ void __launch_bounds__(kThreads) adj_integrate(sph_config c, StepCoun
 }
 
 // ---------------------------------------------------------------- force pairs
-// The pairs are found by the warp-lockstep stencil walk of the forward force
-// pass (warp_pairs): each lane adds its pairs in walk order, so the sums do
-// not depend on which particles share its warp.
+// ---------------------------------------------------------------- candidate lists
+// The neighbour candidate list of a taped step, rebuilt from the tape: the
+// step's start-of-step positions and cell ranges give the same stencil walk,
+// and so the same entries in the same order, as the forward density pass
+// recorded (every neighbour within (1 + margin) h_max).
+template <int DIM>
+__global__ void __launch_bounds__(kThreads) adj_lists(sph_config c, StepCounts k, TapeStep t, WorkPtrs w)
+{
+    const float re2 = energy_list_r2(c);
+    for (uint32_t s = grid_stride_start(); s < k.n; s += grid_stride()) {
+        const float4 pi = t.spos[s];
+        const uint32_t key = t.skey[s];
+        uint3 q;
+        q.x = key % c.ncell[0];
+        q.y = (key / c.ncell[0]) % c.ncell[1];
+        q.z = DIM == 3 ? key / (c.ncell[0] * c.ncell[1]) : 0u;
+        uint32_t nl = 0;
+        auto add = [&](uint32_t j, float4 pj) {   // j != s
+            float dx, dyy, dzz;
+            if (r2_of<DIM>(pj, pi, dx, dyy, dzz) < re2) {
+                if (nl < kNbrListCap) w.nlist[nl_at(w, s, nl)] = j;
+                ++nl;
+            }
+        };
+        auto range = [&](uint32_t b, uint32_t e) {
+            uint32_t j = b;
+            for (; j + 4 <= e; j += 4) {
+                const float4 p0 = t.spos[j], p1 = t.spos[j + 1], p2 = t.spos[j + 2], p3 = t.spos[j + 3];
+                add(j, p0);
+                add(j + 1, p1);
+                add(j + 2, p2);
+                add(j + 3, p3);
+            }
+            for (; j < e; ++j) add(j, t.spos[j]);
+        };
+#pragma unroll 1
+        for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
+#pragma unroll 1
+            for (int dy = -1; dy <= 1; ++dy) {
+                uint32_t b, e;
+                if (!row_range<DIM>(c, t.cell_off, q, dy, dz, b, e)) continue;
+                if (dy == 0 && dz == 0) {
+                    range(b, s);
+                    range(s + 1u, e);
+                } else {
+                    range(b, e);
+                }
+            }
+        w.ncnt[s] = nl;
+    }
+}
+
+// The pairs come from the step's candidate list, filtered by the forward
+// pass's test, or, when a lane's list overflowed, from the warp-lockstep
+// stencil walk (warp_pairs).  Either way each lane adds its pairs in walk
+// order, so the sums do not depend on the path or on which particles share
+// its warp.
 template <int DIM>
 __global__ void __launch_bounds__(kThreads) adj_force(sph_config c, StepCounts k, TapeStep t, WorkPtrs w, AdjPtrs a)
 {
@@ -232,7 +286,26 @@ __global__ void __launch_bounds__(kThreads) adj_force(sph_config c, StepCounts k
             gV += Ddv * aj.w * visc * 0.5f * T;
             gmu += 0.25f * Ddv * VV * T;     // each unordered pair is visited from both ends
         };
-        warp_pairs<DIM>(c, t.cell_off, t.spos, valid, q, smem[wib], accept, pair);
+        const unsigned full = 0xffffffffu;
+        const uint32_t nf = valid && w.nlist ? w.ncnt[s] : 0u;
+        if (__all_sync(full, w.nlist != nullptr && nf <= kNbrListCap)) {
+            const uint32_t m = __reduce_max_sync(full, nf);
+            if (4 < m) prefetch_l2(w.nlist + nl_at(w, s, 4));
+            for (uint32_t kk = 0; kk < m; kk += 4) {
+                if (kk + 8 < m) prefetch_l2(w.nlist + nl_at(w, s, kk + 8));   // two rounds ahead
+                const uint4 t4 = *reinterpret_cast<const uint4 *>(w.nlist + nl_at(w, s, kk));
+                const uint32_t tt[4] = {kk < nf ? t4.x : s, kk + 1 < nf ? t4.y : s, kk + 2 < nf ? t4.z : s,
+                                        kk + 3 < nf ? t4.w : s};
+                float4 pj[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) pj[u] = t.spos[tt[u]];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (kk + u < nf && accept(tt[u], pj[u])) pair(tt[u]);
+            }
+        } else {
+            warp_pairs<DIM>(c, t.cell_off, t.spos, valid, q, smem[wib], accept, pair);
+        }
         if (!valid) continue;
         // p = gas ((rho/rho0)^3 - 1); A = p / rho^2; V = m / rho
         const float rho = ai.x, p = ai.y;
@@ -251,7 +324,8 @@ __global__ void __launch_bounds__(kThreads) adj_force(sph_config c, StepCounts k
 
 // ---------------------------------------------------------------- density pairs
 template <int DIM>
-__global__ void __launch_bounds__(kThreads) adj_density(sph_config c, StepCounts k, TapeStep t, AdjPtrs a)
+__global__ void __launch_bounds__(kThreads) adj_density(sph_config c, StepCounts k, TapeStep t, WorkPtrs w,
+                                                        AdjPtrs a)
 {
     const float skip = c.density_skip_r2;
     for (uint32_t s = grid_stride_start(); s < k.n; s += grid_stride()) {
@@ -295,19 +369,38 @@ __global__ void __launch_bounds__(kThreads) adj_density(sph_config c, StepCounts
             }
             for (; j < e; ++j) visit(j, t.spos[j]);
         };
-#pragma unroll 1
-        for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
-#pragma unroll 1
-            for (int dy = -1; dy <= 1; ++dy) {
-                uint32_t b, e;
-                if (!row_range<DIM>(c, t.cell_off, q, dy, dz, b, e)) continue;
-                if (dy == 0 && dz == 0) {
-                    range(b, s);
-                    range(s + 1u, e);
-                } else {
-                    range(b, e);
-                }
+        // the step's candidate list holds every pair with a term (r^2 below
+        // h_i^2 or h_j^2), in walk order; an overflowed list walks
+        const uint32_t nl = w.nlist ? w.ncnt[s] : kEmpty;
+        if (nl <= kNbrListCap) {
+            uint32_t kk = 0;
+            for (; kk + 4 <= nl; kk += 4) {
+                const uint4 t4 = *reinterpret_cast<const uint4 *>(w.nlist + nl_at(w, s, kk));
+                const float4 p0 = t.spos[t4.x], p1 = t.spos[t4.y], p2 = t.spos[t4.z], p3 = t.spos[t4.w];
+                visit(t4.x, p0);
+                visit(t4.y, p1);
+                visit(t4.z, p2);
+                visit(t4.w, p3);
             }
+            for (; kk < nl; ++kk) {
+                const uint32_t j = w.nlist[nl_at(w, s, kk)];
+                visit(j, t.spos[j]);
+            }
+        } else {
+#pragma unroll 1
+            for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
+#pragma unroll 1
+                for (int dy = -1; dy <= 1; ++dy) {
+                    uint32_t b, e;
+                    if (!row_range<DIM>(c, t.cell_off, q, dy, dz, b, e)) continue;
+                    if (dy == 0 && dz == 0) {
+                        range(b, s);
+                        range(s + 1u, e);
+                    } else {
+                        range(b, e);
+                    }
+                }
+        }
         const uint32_t i = t.sidx[s];
         a.gx_in[i] = make_float4(gx.x, gx.y, DIM == 3 ? gx.z : 0.f, 0.f);
         a.gev_in[i] = a.gevd[s];

@@ -228,6 +228,10 @@ template <int DIM> int backward_impl(sph_handle *h, Rollout *r, float *d_vel0, f
     cudaMemsetAsync(r->gev[p], 0, sizeof(float4) * (nT ? nT : 1), s);
     cudaMemsetAsync(r->param, 0, sizeof(double) * 2 * nscn, s);
     const uint32_t nseg = (r->nsteps + r->every - 1) / r->every;
+    WorkPtrs w = h->w;
+    if (c.walk_only) {   // the same pairs found by the stencil walks
+        w.nlist = w.ncnt = nullptr;
+    }
     for (uint32_t seg = nseg; seg-- > 0;) {
         if (int rc = tape_segment<DIM>(h, r, seg)) return rc;
         for (uint32_t l = seg_len(r, seg); l-- > 0;) {
@@ -242,8 +246,11 @@ template <int DIM> int backward_impl(sph_handle *h, Rollout *r, float *d_vel0, f
             const uint32_t G = grid_for(h, k.n);
             adj_write<DIM><<<G, kThreads, 0, s>>>(c, k, r->tape[l], a);
             adj_integrate<DIM><<<G, kThreads, 0, s>>>(c, k, r->tape[l], a);
-            adj_force<DIM><<<G, kThreads, 0, s>>>(c, k, r->tape[l], h->w, a);
-            adj_density<DIM><<<G, kThreads, 0, s>>>(c, k, r->tape[l], a);
+            // the step's candidate lists, rebuilt from its tape (the working
+            // lists are free during the backward pass)
+            if (w.nlist) adj_lists<DIM><<<G, kThreads, 0, s>>>(c, k, r->tape[l], w);
+            adj_force<DIM><<<G, kThreads, 0, s>>>(c, k, r->tape[l], w, a);
+            adj_density<DIM><<<G, kThreads, 0, s>>>(c, k, r->tape[l], w, a);
             p ^= 1;
         }
     }
