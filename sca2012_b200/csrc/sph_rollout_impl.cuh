@@ -18,6 +18,7 @@ struct Rollout {
     bool valid = false;
     std::vector<TapeStep> tape;
     std::vector<StepCounts> counts;    // of the taped interval
+    StepCounts *dcounts = nullptr;     // the same, written on the device as each step is taped
     int taped_seg = -1;
     float4 *gx[2] = {}, *gv[2] = {}, *gev[2] = {};
     float4 *gx2 = nullptr, *gv2 = nullptr, *gev2 = nullptr, *gxd = nullptr, *gf = nullptr, *gevd = nullptr;
@@ -130,35 +131,45 @@ const char *rollout_unsupported(const sph_config &c)
 }
 
 // One forward step with its topology written into tape slot l.
+// Copies a finished step's sorted-order arrays into tape slot t and its
+// counters into *counts, over the live count the device holds (no host
+// round trip per step).
+__global__ void __launch_bounds__(kThreads) k_tape_record(const Counters *__restrict__ cnt, WorkPtrs w, TapeStep t,
+                                                        uint32_t ncells, StepCounts *counts)
+{
+    const uint32_t n = cnt->n;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        *counts = StepCounts{cnt->n, cnt->n_split, cnt->n_removed, cnt->split_off ? 0u : 1u};
+    for (uint32_t s = grid_stride_start(); s < n; s += grid_stride()) {
+        t.sidx[s] = w.sidx[s]; t.inv[s] = w.inv[s]; t.skey[s] = w.skey[s];
+        t.spos[s] = w.spos[s]; t.svel[s] = w.svel[s]; t.sev[s] = w.sev[s];
+        t.saux[s] = w.saux[s]; t.sacc[s] = w.sacc_n[s];
+        t.spos_n[s] = w.spos_n[s]; t.svel_n[s] = w.svel_n[s]; t.sev_n[s] = w.sev_n[s];
+        t.split_c[s] = w.split_c[s]; t.split_rank[s] = w.split_rank[s];
+        t.removed_c[s] = w.removed_c[s]; t.removed_rank[s] = w.removed_rank[s];
+        t.mpos[s] = w.mpos[s]; t.mvel[s] = w.mvel[s]; t.mev[s] = w.mev[s];
+        if (w.nscenes) t.sscene[s] = w.sscene[s];
+    }
+    for (uint32_t k = grid_stride_start(); k <= ncells; k += grid_stride()) t.cell_off[k] = w.cell_off[k];
+}
+
 template <int DIM> int taped_step(sph_handle *h, Rollout *r, uint32_t l)
 {
     TapeStep &t = r->tape[l];
-    const uint32_t n = read_n(h);
     cudaStream_t s = h->stream;
-    cudaMemsetAsync(t.merge_to, 0xff, sizeof(uint32_t) * (n ? n : 1), s);
+    // merge leaders fill merge_to; n_ub bounds the live count
+    cudaMemsetAsync(t.merge_to, 0xff, sizeof(uint32_t) * (h->n_ub ? h->n_ub : 1), s);
     const WorkPtrs saved = h->w;
     h->w.merge_to = t.merge_to;
     h->w.mvs = t.mvs;
     h->w.wall = t.wall;
     const int p = h->cur;
+    const uint32_t nub = h->n_ub;
     const int rc = run_step<DIM>(h);
     h->w = saved;
     if (rc) return rc;
-    const WorkPtrs &w = h->w;
-    d2d(t.sidx, w.sidx, n, s); d2d(t.inv, w.inv, n, s); d2d(t.skey, w.skey, n, s);
-    d2d(t.cell_off, w.cell_off, (size_t)h->ncells + 1, s);
-    d2d(t.spos, w.spos, n, s); d2d(t.svel, w.svel, n, s); d2d(t.sev, w.sev, n, s);
-    d2d(t.saux, w.saux, n, s); d2d(t.sacc, w.sacc_n, n, s);
-    d2d(t.spos_n, w.spos_n, n, s); d2d(t.svel_n, w.svel_n, n, s); d2d(t.sev_n, w.sev_n, n, s);
-    d2d(t.split_c, w.split_c, n, s); d2d(t.split_rank, w.split_rank, n, s);
-    d2d(t.removed_c, w.removed_c, n, s); d2d(t.removed_rank, w.removed_rank, n, s);
-    d2d(t.mpos, w.mpos, n, s); d2d(t.mvel, w.mvel, n, s); d2d(t.mev, w.mev, n, s);
-    if (w.nscenes) d2d(t.sscene, w.sscene, n, s);
-    Counters c0;
-    cudaMemcpyAsync(&c0, &h->cnt[p], sizeof(Counters), cudaMemcpyDeviceToHost, s);
-    cudaStreamSynchronize(s);
-    if (c0.n != n) { h->err = "rollout: particle count changed during a taped step"; return SPH_ERR_INVALID; }
-    r->counts[l] = StepCounts{c0.n, c0.n_split, c0.n_removed, c0.split_off ? 0u : 1u};
+    k_tape_record<<<grid_for(h, std::max(nub, h->ncells + 1)), kThreads, 0, s>>>(h->cnt + p, h->w, t, h->ncells,
+                                                                                r->dcounts + l);
     return cuda_check(h, "rollout: taped step");
 }
 
@@ -173,8 +184,13 @@ template <int DIM> int tape_segment(sph_handle *h, Rollout *r, uint32_t seg)
     if (r->taped_seg == (int)seg) return SPH_OK;
     r->taped_seg = -1;
     if (int rc = restore_ckpt(h, r, seg)) return rc;
-    for (uint32_t l = 0; l < seg_len(r, seg); ++l)
+    const uint32_t len = seg_len(r, seg);
+    for (uint32_t l = 0; l < len; ++l)
         if (int rc = taped_step<DIM>(h, r, l)) return rc;
+    // the interval's step counters, read once
+    cudaMemcpyAsync(r->counts.data(), r->dcounts, sizeof(StepCounts) * len, cudaMemcpyDeviceToHost, h->stream);
+    cudaStreamSynchronize(h->stream);
+    if (int rc = cuda_check(h, "rollout: taped interval")) return rc;
     r->taped_seg = (int)seg;
     return SPH_OK;
 }
@@ -389,6 +405,7 @@ int sph_rollout_forward(sph_handle *h, uint32_t nsteps, uint32_t every)
         r->tape.resize(slots);
         r->tape_slots = slots;
         for (auto &t : r->tape) rc |= alloc_tape(h, r, t);
+        rc |= ralloc(h, r, &r->dcounts, slots);
         for (int q = 0; q < 2; ++q) {
             rc |= ralloc(h, r, &r->gx[q], r->cap); rc |= ralloc(h, r, &r->gv[q], r->cap);
             rc |= ralloc(h, r, &r->gev[q], r->cap);
