@@ -296,12 +296,9 @@ __global__ void __launch_bounds__(kThreads) adj_force(sph_config c, StepCounts k
                 const uint4 t4 = *reinterpret_cast<const uint4 *>(w.nlist + nl_at(w, s, kk));
                 const uint32_t tt[4] = {kk < nf ? t4.x : s, kk + 1 < nf ? t4.y : s, kk + 2 < nf ? t4.z : s,
                                         kk + 3 < nf ? t4.w : s};
-                float4 pj[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) pj[u] = t.spos[tt[u]];
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
-                    if (kk + u < nf && accept(tt[u], pj[u])) pair(tt[u]);
+                    if (kk + u < nf && accept(tt[u], t.spos[tt[u]])) pair(tt[u]);
             }
         } else {
             warp_pairs<DIM>(c, t.cell_off, t.spos, valid, q, smem[wib], accept, pair);
