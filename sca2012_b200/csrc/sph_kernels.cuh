@@ -9,8 +9,11 @@
 //   sorted working copies, in cell-key order, that the neighbour loops read
 //   contiguously: spos/svel/sev (gathered), saux = (rho, p, p/rho^2, m/rho),
 //   and the post-integration spos_n/svel_n/sev_n/sacc_n, ssurf, senergy;
-//   per-particle neighbour candidate lists (nlist), written by the density
-//   pass and read by the force and energy passes.
+//   a force neighbour's values in two 16-byte records fnb_a = (x, y, z,
+//   p/rho^2) and fnb_b = (m/rho signed by level, ev), written by density;
+//   per-particle neighbour candidate lists (nlist, rows of four-entry
+//   chunks), written by the density pass and read by the force and energy
+//   passes.
 // Cell key = z*R*C + y*R + x with x = floor(pos / cell) in FP32, exactly the
 // reference's calc_grid_pos/calc_grid_hash (SPH-3D-2/sph_system.cu:18-32).
 // Neighbour search visits the 3 (2D) or 9 (3D) rows of x-adjacent cells; in
