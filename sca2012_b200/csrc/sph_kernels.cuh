@@ -512,7 +512,9 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
                 jpk = (lj ? jspk1 : jspk0) * jkr * jkr;
                 jvk = (lj ? jvis1 : jvis0) * jkr;
             }
-            const float tp = (lj ? mimj1 : mimj0) * (ai.z + a.w) * (ipk + jpk) * 0.5f / r;
+            // 1/r from the approximate reciprocal square root of r^2 (the h - r
+            // decisions above keep the IEEE square root)
+            const float tp = (lj ? mimj1 : mimj0) * (ai.z + a.w) * (ipk + jpk) * 0.5f * rsqrtf(r2);
             const float tv = (ai.w * mrj) * visc * (ivk + jvk) * 0.5f;
             fx += -rx * tp + (b.y - evi.x) * tv;
             fy += -ry * tp + (b.z - evi.y) * tv;
