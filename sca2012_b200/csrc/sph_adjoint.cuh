@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(kThreads) adj_force(sph_config c, StepCounts k
             const float4 aj = t.saux[j], evj = t.sev[j], gfj = a.gf[j];
             const float mm = mi * c.mass[lj];
             const float Cp = mm * (ai.z + aj.z) * 0.5f;
-            const float ir = 1.0f / r;
+            const float ir = rsqrtf(r2);   // 1/r as the forward pass takes it
             const float tp = Cp * S * ir, dtp = Cp * (dS - S * ir) * ir;
             const float VV = ai.w * aj.w;
             const float tv = VV * visc * 0.5f * T, dtv = VV * visc * 0.5f * dT;
