@@ -402,13 +402,14 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restri
         auto range = [&](uint32_t b, uint32_t e) {
             uint32_t t = b;
             for (; t + 4 <= e; t += 4) {
-                const float4 p0 = w.spos[t], p1 = w.spos[t + 1], p2 = w.spos[t + 2], p3 = w.spos[t + 3];
+                const float4 p0 = __ldg(w.spos + t), p1 = __ldg(w.spos + t + 1), p2 = __ldg(w.spos + t + 2),
+                             p3 = __ldg(w.spos + t + 3);
                 add(t, p0);
                 add(t + 1, p1);
                 add(t + 2, p2);
                 add(t + 3, p3);
             }
-            for (; t < e; ++t) add(t, w.spos[t]);
+            for (; t < e; ++t) add(t, __ldg(w.spos + t));
         };
 #pragma unroll 1
         for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
