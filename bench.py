@@ -21,7 +21,10 @@ no data-parallel split without a halo exchange): weak scaling, value = sum
 of particle-steps / max over ranks of the timed duration.
 
 --impl reference times the CPU oracle (the FP64 port of the reference step)
-on the host cores on the same workload, rank 0 only.
+on the host cores on the same workload, rank 0 only.  That arm loads no part
+of the package's CUDA library: its configuration comes from the oracle's
+restatement of the preset (oracle/presets.py, checked byte for byte against
+the library's) and its particles from the numpy scene generator.
 """
 import argparse
 import json
@@ -49,7 +52,7 @@ STAGE_BYTES = {
     "hash": 16 + 4 + 4 + 4,                  # pos in; key, slot out; count atomics
     "scatter": 4 + 4 + 4 + 4,                # key, slot, offset in; index out
     "reorder": 4 + 4 + 48 + 4 + 4 + 4,       # index, key, pos/vel/ev in; sidx, skey, inv out
-    "density": 16 + 16 + 4,                  # pos in; (rho, p, p/rho^2, m/rho), nbr out
+    "density": 16 + 4 + 8,                   # pos, m in; rho, p out (the unfused figure per stage)
     "force_integrate": 16 * 4 + 16 * 4 + 4,  # pos, ev, aux, vel in; pos, vel, ev, acc, surface out
     "energy_split": 16 + 16 + 4 + 16 + 4 + 4 + 4 + 4 + 4,  # new pos, vel, surf, aux, nbr, idx; energy, flags
     "write": 4 * 16 + 16 + 4 * 4 + 4 * 4 + 4 * 16 + 5 * 4,  # sorted state + flags in; canonical state out
@@ -169,6 +172,28 @@ def load_workload(seed):
     return cfg, pos, vel, lvl
 
 
+def load_workload_host_only(seed):
+    """The same workload for the CPU reference arm without the package: the
+    configuration from the oracle's restatement of the preset, the particles
+    from the scene generator's file loaded on its own (plain numpy).  Nothing
+    of the CUDA library is loaded."""
+    import importlib.util
+    from oracle import presets
+    spec = importlib.util.spec_from_file_location("_bench_scenes", os.path.join(ROOT, "sca2012_b200", "scenes.py"))
+    scenes = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(scenes)
+    cfg = presets.preset(presets.PRESET_DAM_3D4)
+    pos, vel, lvl = scenes.dam_3d4(cfg, seed=seed)
+    return cfg, pos, vel, lvl
+
+
+def workload_config(cfg, n0):
+    """The `config` of both arms' JSON lines: what defines the workload."""
+    return {"workload": WORKLOAD, "particles_initial": int(n0),
+            "cells": int(cfg.ncell[0] * cfg.ncell[1] * cfg.ncell[2]),
+            "max_particle": int(cfg.max_particle)}
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -177,15 +202,27 @@ def measured_peaks():
     return 6650.0, "fallback 6.65 TB/s"
 
 
-def profiled_traffic(stage):
-    """Per-launch DRAM bytes of `stage` from the committed ncu summary, if any."""
+def profiled_counters(stage):
+    """Per-launch DRAM bytes and warp instructions of `stage` from the
+    committed ncu summary, with the particle count of that launch (None where
+    absent)."""
     path = os.path.join(ROOT, "profiles", f"{stage}_dam3d4.txt")
     if not os.path.exists(path):
-        return None, None
+        return None, None, None
     txt = open(path).read()
     m = re.search(r"traffic_bytes_per_launch_full:\s*([0-9.eE+]+)", txt)
+    i = re.search(r"smsp__inst_executed.sum\s+([0-9.]+) M", txt)
     n = re.search(r"particles_full:\s*([0-9]+)", txt)
-    return (float(m.group(1)) if m else None), (int(n.group(1)) if n else None)
+    return ((float(m.group(1)) if m else None), (float(i.group(1)) * 1e6 if i else None),
+            (int(n.group(1)) if n else None))
+
+
+def issue_fraction(inst, n_prof, n_now, ms, sm_mhz, sms=148):
+    """Warp instructions issued (scaled by particle count) over the issue slots
+    of the launch: SMs x 4 schedulers x SM clock x duration."""
+    if not (inst and n_prof and ms and sm_mhz):
+        return None
+    return inst * (n_now / n_prof) / (sms * 4 * sm_mhz * 1e6 * ms * 1e-3)
 
 
 def cpu_baseline(cfg, pos, vel, lvl, steps, threads=None):
@@ -301,12 +338,24 @@ def run_ours(args, rank, world, local_rank):
     peak, peak_src = measured_peaks()
     alg = STAGE_BYTES.get(top, 0) * n_avg
     achieved = alg / (stage_avg[top] * 1e-3) / 1e9
-    traffic_full, n_full = profiled_traffic(top)
+    traffic_full, _, n_full = profiled_counters(top)
     traffic = traffic_full * (n_avg / n_full) if traffic_full and n_full else None
     # the three neighbour loops together against their compulsory bytes
-    # (density 28 + force 64 + energy 36 = 128 B per particle-step)
+    # (density 28 + force 64 + energy 36 = 128 B per particle-step), and each
+    # against the two bounds it can hit: HBM bytes and instruction issue
     nl_ms = sum(stage_avg.get(k, 0.0) for k in ("density", "force_integrate", "energy_split"))
     nl_gbs = 128.0 * n_avg / (nl_ms * 1e-3) / 1e9 if nl_ms else None
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    per_kernel = {}
+    for k, nb in (("density", 28), ("force_integrate", 64), ("energy_split", 36)):
+        if k not in stage_avg:
+            continue
+        tr, inst, n_p = profiled_counters(k)
+        a = nb * n_avg / (stage_avg[k] * 1e-3) / 1e9
+        per_kernel[k] = {"ms": stage_avg[k], "algorithmic_bytes_per_particle": nb, "achieved_gbs": a,
+                         "hbm_frac": a / peak,
+                         "dram_traffic_per_launch": tr * (n_avg / n_p) if tr and n_p else None,
+                         "issue_frac": issue_fraction(inst, n_p, n_avg, stage_avg[k], sm_mhz)}
 
     # --- plain (non-adaptive) step on the same state, for the "vs plain" ratio
     plain = cfg.copy()
@@ -393,9 +442,8 @@ def run_ours(args, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "particles_initial": n0,
-                       "particles_timed_mean": ps / args.steps / world,
-                       "cells": int(cfg.ncell[0] * cfg.ncell[1] * cfg.ncell[2]),
+            "config": workload_config(cfg, n0),
+            "timing": {"particles_timed_mean": ps / args.steps / world,
                        "l2": "flushed (256 MB write) between timed steps",
                        "launch": "CUDA graph replay per step (surface steps launch directly)",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
@@ -411,7 +459,12 @@ def run_ours(args, rank, world, local_rank):
                                   "(force, energy): the HBM fraction is low by design"),
                          "neighbour_loops": {"stages": ["density", "force_integrate", "energy_split"],
                                              "bytes_per_particle": 128, "ms": nl_ms, "achieved": nl_gbs,
-                                             "frac": nl_gbs / peak if nl_gbs else None}},
+                                             "frac": nl_gbs / peak if nl_gbs else None,
+                                             "per_kernel": per_kernel,
+                                             "issue_frac_note": ("ncu smsp__inst_executed.sum of the committed "
+                                                                 "profiles/<kernel>_dam3d4.txt, scaled by particle "
+                                                                 "count, / (148 SMs x 4 x median SM clock x live "
+                                                                 "kernel time)")}},
             "stages_ms": stage_avg,
             "tuning": tuning,
             "conserved": conserved,
@@ -661,7 +714,7 @@ def rollout_bench(args):
 def run_reference(args, rank):
     if rank != 0:
         return None
-    cfg, pos, vel, lvl = load_workload(args.seed)
+    cfg, pos, vel, lvl = load_workload_host_only(args.seed)
     from oracle import oracle as O
     st = dict(pos=pos, vel=vel, level=lvl)
     cap = len(pos) * 4
@@ -679,7 +732,7 @@ def run_reference(args, rank):
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "particles_initial": len(pos)},
+            "config": workload_config(cfg, len(pos)),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": O.get_threads(), "kind": "port",
                              "sample": f"{args.steps} full steps of the workload, FP64 oracle, OpenMP, "
                                        f"after {min(args.warmup, 1)} warm-up step(s)"},

@@ -328,7 +328,10 @@ int sph_readback_wait(sph_handle *h);
  * Scratch lives in one fixed static device array: at most
  * SPH_NOALLOC_MAX_PARTICLES particles and SPH_NOALLOC_MAX_CELLS cells, larger
  * inputs return SPH_ERR_RANGE.  The first call on a device looks up the
- * array's device address; make it before any stream capture begins.  Calls
+ * array's device address; make it before any stream capture begins.  The
+ * address is kept for the life of the process: after cudaDeviceReset on a
+ * device it is stale, so do not call this entry point on that device again
+ * in the same process.  Calls
  * share the array, so calls that overlap on the GPU race.  Asynchronous on
  * `stream` (a cudaStream_t, NULL = default stream).
  */

@@ -6,10 +6,14 @@
 # v in {2d, 3d2, 3d4}; the _mc library exists for the 3D variants only.
 # The only project-written code compiled in is oracle/ref_shim/cutil_math.h
 # (stand-in for the retired SDK header) and the two drivers.
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh REFERENCE_ROOT   (or SCA2012_REFERENCE=REFERENCE_ROOT)
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${SCA2012_REFERENCE:-}}"
+if [ -z "$REF" ]; then
+  echo "build_ref: no reference root given (argument or SCA2012_REFERENCE); keeping existing oracle/_ref" >&2
+  exit 0
+fi
 OUT="$HERE/_ref"
 mkdir -p "$OUT"
 if [ ! -d "$REF/SPH-3D-2" ]; then

@@ -23,9 +23,24 @@ class RefTopo(C.Structure):
         (k, C.POINTER(C.c_float)) for k in ("x_rec", "v_rec", "ev_rec")]
 
 
-def _cfg_type():
-    from sca2012_b200._abi import Config, StateView, DebugView
-    return Config, StateView, DebugView
+def abi():
+    """The ctypes mirror of sph.h's structs (sca2012_b200/_abi.py).  When the
+    package is already imported its module is used, so that structs built by
+    either side have the same types; otherwise the file is loaded on its own,
+    without importing the package or loading its CUDA library."""
+    import sys
+    mod = sys.modules.get("sca2012_b200._abi")
+    if mod is not None:
+        return mod
+    mod = sys.modules.get("_oracle_abi_mirror")
+    if mod is None:
+        import importlib.util
+        path = os.path.join(os.path.dirname(HERE), "sca2012_b200", "_abi.py")
+        spec = importlib.util.spec_from_file_location("_oracle_abi_mirror", path)
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["_oracle_abi_mirror"] = mod
+        spec.loader.exec_module(mod)
+    return mod
 
 
 def load():
@@ -34,9 +49,10 @@ def load():
         return _lib
     if not os.path.exists(LIB_PATH):
         raise RuntimeError("oracle/libsph_oracle.so not built (make -C oracle)")
-    Config, StateView, DebugView = _cfg_type()
+    A = abi()
+    StateView, DebugView = A.StateView, A.DebugView
     lib = C.CDLL(LIB_PATH)
-    PC = C.POINTER(Config)
+    PC = C.c_void_p   # sph_config*, from any mirror of the struct (passed by byref)
     U = C.POINTER(C.c_uint32)
     F = C.POINTER(C.c_float)
     D = C.POINTER(C.c_double)
@@ -55,9 +71,8 @@ def load():
                                 C.POINTER(DebugView)]
     lib.oracle_step.restype = C.c_int64
     lib.oracle_density_grid.argtypes = [PC, C.c_uint32, F, U, U, U, U, D, D]
-    from sca2012_b200._abi import LossGrid
     PT = C.POINTER(RefTopo)
-    PG = C.POINTER(LossGrid)
+    PG = C.POINTER(A.LossGrid)
     lib.ref_rollout_forward.argtypes = [PC, PT, C.c_uint32, C.c_uint32, D, D, C.c_double, C.c_double, PG, D, D]
     lib.ref_rollout_forward.restype = C.c_double
     lib.ref_rollout_grad.argtypes = [PC, PT, C.c_uint32, C.c_uint32, D, D, C.c_double, C.c_double, PG, D,
@@ -176,8 +191,7 @@ _STATE_F = ("pos", "vel", "ev", "acc", "dens", "press", "energy", "surface")
 
 
 def _view(st, n, keep):
-    from sca2012_b200._abi import StateView
-    v = StateView()
+    v = abi().StateView()
     v.n = n
     for k in _STATE_F + ("level", "interior"):
         a = st.get(k)
@@ -232,7 +246,7 @@ def adapt(cfg, st, nbr, idx, cs, ce, cap=None):
 
 def step(cfg, st, cap=None):
     """One whole oracle step on a state dict; returns (new state, debug)."""
-    from sca2012_b200._abi import DebugView
+    DebugView = abi().DebugView
     lib = load()
     n = len(st["pos"])
     cap = cap or max(n * (4 if cfg.split_ways == 4 else 2), 1)
@@ -277,7 +291,7 @@ class Rollout64:
     dicts of steps 0..T-1."""
 
     def __init__(self, cfg, topo, grid_n, origin, spacing, target):
-        from sca2012_b200._abi import LossGrid
+        LossGrid = abi().LossGrid
         self.lib = load()
         self.cfg = cfg
         self.keep = topo

@@ -42,13 +42,15 @@ def build_oracle():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
 
 
-def build_reference_oracle():
-    """Compiles the reference itself into oracle/_ref when its tree is present."""
-    ref = "/root/reference"
+def build_reference_oracle(ref=None):
+    """Compiles the reference itself into oracle/_ref when its source tree is
+    given (`ref`, else the SCA2012_REFERENCE environment variable) and the
+    libraries are not built yet."""
+    ref = ref or os.environ.get("SCA2012_REFERENCE", "")
     script = os.path.join(ROOT, "oracle", "build_ref.sh")
     have = all(os.path.exists(os.path.join(ROOT, "oracle", "_ref", f"libref_{v}_gpu.so"))
                for v in ("2d", "3d2", "3d4"))
-    if os.path.isdir(ref) and not have:
+    if ref and os.path.isdir(ref) and not have:
         subprocess.run(["bash", script, ref], check=True)
 
 

@@ -16,7 +16,10 @@
 // GPU can reach host memory, silently touch the wrong memory.  The first call
 // on each device therefore looks up the real device address with
 // cudaGetSymbolAddress (with that device current) and caches it; make that
-// first call before any stream capture begins.  All calls share the array and
+// first call before any stream capture begins.  The cached address lives as
+// long as the process; cudaDeviceReset unloads the module that holds the array,
+// after which the cached address is stale and this entry point must not be
+// called on that device again.  All calls share the array and
 // it keeps the last call's contents: the counters that must start at zero are
 // cleared by every call, and calls that overlap on the GPU (two streams, or
 // two host threads) race on it.
@@ -115,7 +118,11 @@ __global__ void __launch_bounds__(kThreads) na_scatter(uint32_t n, const uint32_
     for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) tmp[off[key[i]] + slot[i]] = i;
 }
 
-// stable order inside each cell: rank by particle index among the cell's members
+// stable order inside each cell: rank by particle index among the cell's members.
+// A particle compares itself with every member of its cell, so the cost is
+// quadratic in a cell's population; with at most SPH_NOALLOC_MAX_PARTICLES
+// particles and cells of an SPH kernel length (tens of members) that stays
+// small, but a caller that piles many particles into one cell pays for it.
 __global__ void __launch_bounds__(kThreads) na_rank(uint32_t n, const uint32_t *__restrict__ key,
                                                    const uint32_t *__restrict__ off, const uint32_t *__restrict__ tmp,
                                                    uint32_t *__restrict__ key_out, uint32_t *__restrict__ index_out)

@@ -18,10 +18,20 @@ Tolerances (stated once, used everywhere):
     code decides (the surface-tension switch, a wall) are reported as
     ambiguous and excluded from the value comparison of that stage.
 """
+import json
+import os
+
 import numpy as np
 
 RTOL = 1e-5
 FLOOR = 1.0
+
+# One record per check_close call: how many particles were compared, how
+# many were held to the field's RMS instead of their own value (|x64| below
+# FLOOR * rms), how many were excluded as ambiguous, and the largest error
+# against each particle's own value among the compared ones.  Written as JSON
+# lines to $SPH_PARITY_REPORT when that is set.
+REPORT = []
 
 
 def norm_rows(a):
@@ -54,11 +64,25 @@ def check_close(name, x, ref, mask=None, rtol=RTOL, floor=FLOOR):
     rs = np.where(nr[:, None] if ref.ndim > 1 else nr, 0, ref)
     e = rel_err(xs, rs, floor)
     e = np.where(ok, e, 0.0)
+    r = norm_rows(rs)
+    rms = np.sqrt(np.mean(r[ok] ** 2)) if ok.any() else 0.0
+    below = ok & (r < floor * rms)
+    own = np.where(ok & (r > 0), norm_rows(xs - rs) / np.where(r > 0, r, 1.0), 0.0)
+    rec = {"name": name, "compared": int(ok.sum()), "held_to_rms": int(below.sum()),
+           "excluded_ambiguous": int((~sel).sum()), "non_finite_matched": int((sel & nr).sum()),
+           "max_err_bound": float(e.max(initial=0.0)),
+           "max_err_own_value_above_rms": float(np.where(below, 0.0, own).max(initial=0.0))}
+    REPORT.append(rec)
+    path = os.environ.get("SPH_PARITY_REPORT")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps(rec) + "\n")
     worst = int(np.argmax(e)) if len(e) else 0
     assert e.max(initial=0.0) <= rtol, (
         f"{name}: max rel err {e.max():.3e} > {rtol:.0e} at particle {worst} "
-        f"(got {x[worst]}, ref {ref[worst]})")
-    return float(e.max(initial=0.0))
+        f"(got {x[worst]}, ref {ref[worst]}); {rec['held_to_rms']} of {rec['compared']} held to the RMS, "
+        f"{rec['excluded_ambiguous']} excluded")
+    return rec["max_err_bound"]
 
 
 def check_equal(name, x, ref):

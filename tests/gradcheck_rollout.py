@@ -25,17 +25,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--every", type=int, default=20)
-    ap.add_argument("--block", type=int, default=32)
-    ap.add_argument("--dirs", type=int, default=64)
-    ap.add_argument("--eps", type=float, default=1e-6)
-    ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--out", default=None)
-    a = ap.parse_args()
-
+def gradcheck(steps=200, every=20, block=32, dirs=64, eps=1e-6, seed=0):
+    """Runs the check and returns its statistics (the JSON line's dict);
+    tests/test_gpu_gradcheck_full.py calls it with 8 directions."""
+    a = argparse.Namespace(steps=steps, every=every, block=block, dirs=dirs, eps=eps, seed=seed)
     import sca2012_b200 as sph
     from sca2012_b200 import scenes
     from oracle import oracle as O
@@ -135,6 +128,23 @@ def main():
         "seconds": {"gpu_forward_backward": t_gpu, "fp64_adjoint": t_ref, "fp64_fd": t_fd},
         "omp_threads": O.get_threads(),
     }
+    out["dir_rel_gpu_vs_fd"] = rel_gpu.tolist()
+    out["dir_err_over_grad_norm"] = nrm_gpu.tolist()
+    out["dir_abs_fd_over_grad_norm"] = (np.abs(d[:, 2]) / gnorm).tolist()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--every", type=int, default=20)
+    ap.add_argument("--block", type=int, default=32)
+    ap.add_argument("--dirs", type=int, default=64)
+    ap.add_argument("--eps", type=float, default=1e-6)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args()
+    out = gradcheck(a.steps, a.every, a.block, a.dirs, a.eps, a.seed)
     line = json.dumps(out)
     print(line, flush=True)
     if a.out:

@@ -1,0 +1,36 @@
+"""The differentiable rollout's gradient at full size, on the GPU: 32,768
+particles (32^3 block), 200 steps with checkpoints every 20, two-way split
+and merge on, the 32^3 density-grid loss (tests/gradcheck_rollout.py has
+the workload).  The GPU gradient (FP32 forward and adjoint) is compared with
+FP64 central finite differences (eps 1e-6) of the FP64 host replay on 8
+random unit directions in (initial velocities, viscosity, stiffness) and on
+viscosity and stiffness alone, and with the FP64 replay's own adjoint.
+
+Bound: within 1e-3 relative of the finite difference for every direction
+whose finite difference is at least 1e-3 of the gradient's norm, and within
+1e-5 of the gradient's norm for every direction (a direction nearly
+orthogonal to the gradient has a tiny finite difference whose relative error
+says nothing about the gradient)."""
+import os
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_full_size_rollout_gradient(gpu):
+    from oracle import oracle as O
+    from tests.gradcheck_rollout import gradcheck
+    O.set_threads(os.cpu_count() or 1)
+    out = gradcheck(steps=200, every=20, block=32, dirs=8, eps=1e-6, seed=0)
+    print({k: v for k, v in out.items() if not isinstance(v, list)})
+    assert out["particles_initial"] == 32768 and out["splits"] > 0 and out["merge_members"] > 0
+    assert out["loss_rel"] < 1e-4
+    assert out["d_vel0_rel_vs_fp64_adjoint"] < 1e-3
+    for name in ("viscosity", "gas_constant"):
+        assert out["params"][name]["rel_gpu_vs_fd"] < 1e-3, (name, out["params"][name])
+    for rel, err_g, fd_g in zip(out["dir_rel_gpu_vs_fd"], out["dir_err_over_grad_norm"],
+                                out["dir_abs_fd_over_grad_norm"]):
+        assert err_g < 1e-5
+        if fd_g >= 1e-3:
+            assert rel < 1e-3

@@ -21,6 +21,10 @@ def _obstacles(c):
     c.push_left = 1          # push force (SPH-3D-2/sph_system.cu:229-236)
 
 
+def _push_right(c):
+    c.push_right = 1         # the 3D-4 push force from the right (SPH-3D-4/sph_system.cu:236-242)
+
+
 def _mouse(c):
     c.extern_force_on = 1    # 2D mouse force (SPH-2D/sph_system.cu:781-789)
     c.extern_click[0], c.extern_click[1] = 8.0, 8.0
@@ -34,6 +38,9 @@ CASES = {
     "dam_2d": (sph.PRESET_DAM_2D, scenes.dam_2d, 3),
     "dam_3d2_small": (sph.PRESET_DAM_3D2, lambda c: scenes.block_3d(c, (24, 24, 12), 0.01, seed=3), 3),
     "ref_3d2_obstacles": (sph.PRESET_REF_3D2, scenes.ref_box_3d2, 8, _obstacles),
+    # the right third of the 3D-4 slab, where the push from the right acts (x > 2W/3)
+    "ref_3d4_push_right": (sph.PRESET_REF_3D4, lambda c: _crop_right(scenes.ref_box_3d4(c), 30.0), 4,
+                           _push_right),
     "ref_2d_mouse": (sph.PRESET_REF_2D, scenes.ref_init_2d, 10, _mouse),
     # the benchmark workload at full size: 1,114,112 particles, four-way
     "dam_3d4_full": (sph.PRESET_DAM_3D4, scenes.dam_3d4, 2),
@@ -46,6 +53,12 @@ def _crop(scene, xmax):
     return pos[m], vel[m], lvl[m]
 
 
+def _crop_right(scene, xmin):
+    pos, vel, lvl = scene
+    m = pos[:, 0] > xmin
+    return pos[m], vel[m], lvl[m]
+
+
 def _cfg(preset, split, merge, n, extra=None):
     c = sph.preset(preset)
     c.use_split = int(split)
@@ -54,6 +67,22 @@ def _cfg(preset, split, merge, n, extra=None):
     if extra:
         extra(c)
     return c
+
+
+def step_pair(s, cfg_on, cfg_off, s0):
+    """From state s0: one step with split/merge off, then the same step with
+    them on (the solver is left after the second)."""
+    s.set_config(cfg_off)
+    s.set_state(s0)
+    s.step(1)
+    assert s.sync_status() == 0
+    s1 = s.get_state()
+    dbg = s.get_debug()
+    s.set_config(cfg_on)
+    s.set_state(s0)
+    s.step(1)
+    assert s.sync_status() == 0
+    return s1, dbg, s.get_state(), s.get_debug()
 
 
 def run_case(name):
@@ -68,27 +97,49 @@ def run_case(name):
     s.step(warm)
     assert s.sync_status() == 0
     s0 = s.get_state()
-    # --- step with split/merge off
-    s.set_config(cfg_off)
-    s.set_state(s0)
-    s.step(1)
-    assert s.sync_status() == 0
-    s1 = s.get_state()
-    dbg = s.get_debug()
-    # --- same step with split/merge on
-    s.set_config(cfg_on)
-    s.set_state(s0)
-    s.step(1)
-    assert s.sync_status() == 0
-    s1_on = s.get_state()
-    dbg_on = s.get_debug()
+    s1, dbg, s1_on, dbg_on = step_pair(s, cfg_on, cfg_off, s0)
     s.close()
     return cfg_on, cfg_off, s0, s1, dbg, s1_on, dbg_on
 
 
 @pytest.mark.parametrize("name", list(CASES))
 def test_step_parity(name, gpu):
-    cfg_on, cfg, s0, s1, dbg, s1_on, dbg_on = run_case(name)
+    verify_step(name, *run_case(name))
+
+
+# Per-step parity deep into the configured runs: the GPU advances the whole
+# run; before each checked step its FP32 state is taken and that step is
+# checked stage by stage against the oracle fed that state.
+DEEP = {
+    # 2D plain dam break, 4,096 particles, no adaptivity, the 1,000-step run
+    "dam_2d_run": (sph.PRESET_DAM_2D, scenes.dam_2d, 0, (1, 250, 500, 1000)),
+    # 3D two-way dam break at full size (131,072 particles), split and merge
+    # on, the 500-step run
+    "dam_3d2_run": (sph.PRESET_DAM_3D2, scenes.dam_3d2, 1, (1, 100, 300, 500)),
+}
+
+
+@pytest.mark.parametrize("name", list(DEEP))
+def test_run_parity(name, gpu):
+    preset, scene, adapt, checks = DEEP[name]
+    pos, vel, lvl = scene(sph.preset(preset), seed=0)
+    cfg_on = _cfg(preset, adapt, adapt, len(pos))
+    cfg_off = _cfg(preset, 0, 0, len(pos))
+    s = sph.Solver(cfg_on)
+    s.set_debug(True)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    done = 0
+    for k in checks:
+        s.step(k - 1 - done)
+        assert s.sync_status() == 0
+        s0 = s.get_state()
+        s1, dbg, s1_on, dbg_on = step_pair(s, cfg_on, cfg_off, s0)
+        done = k
+        verify_step(f"{name}@{k}", cfg_on, cfg_off, s0, s1, dbg, s1_on, dbg_on)
+    s.close()
+
+
+def verify_step(name, cfg_on, cfg, s0, s1, dbg, s1_on, dbg_on):
     n = len(s0["pos"])
     assert dbg["n"] == n and len(s1["pos"]) == n
 
@@ -102,23 +153,23 @@ def test_step_parity(name, gpu):
     # (b) density / pressure / neighbour counts
     dens, press, nbr = O.density(cfg, s0["pos"], s0["level"], idx, cs, ce)
     check_equal("neighbour counts", dbg["nbr_count"], nbr)
-    check_close("density", s1["dens"], dens)
-    check_close("pressure", s1["press"], press)
+    check_close(f"{name}/density", s1["dens"], dens)
+    check_close(f"{name}/pressure", s1["press"], press)
 
     # (c) forces + integration
     acc, surf, amb = O.force(cfg, s0["pos"], s0["ev"], s0["level"], dens, press, idx, cs, ce)
     p64, v64, e64, a64, amb2 = O.integrate(cfg, s0["pos"], s0["vel"], s0["ev"], s0["level"], acc, dens)
     ok = ~(amb | amb2)
-    check_close("surface |grad c|", s1["surface"], surf)
-    check_close("acceleration", s1["acc"], a64, ok)
-    check_close("velocity", s1["vel"], v64, ok)
-    check_close("eval velocity", s1["ev"], e64, ok)
-    check_close("position", s1["pos"], p64, ok)
+    check_close(f"{name}/surface |grad c|", s1["surface"], surf)
+    check_close(f"{name}/acceleration", s1["acc"], a64, ok)
+    check_close(f"{name}/velocity", s1["vel"], v64, ok)
+    check_close(f"{name}/eval velocity", s1["ev"], e64, ok)
+    check_close(f"{name}/position", s1["pos"], p64, ok)
 
     # (d) wavelet energy on the stale lists with the GPU's new positions
     en, tv = O.energy(cfg, s1["pos"], s1["vel"], s0["level"], idx, cs, ce)
-    check_close("energy", s1["energy"], en)
-    check_close("trans_vel", dbg["trans_vel"], tv)
+    check_close(f"{name}/energy", s1["energy"], en)
+    check_close(f"{name}/trans_vel", dbg["trans_vel"], tv)
 
     # (e) split + merge + compaction from the same post-energy state
     pre = {k: s1[k] for k in ("pos", "vel", "ev", "acc", "dens", "press", "energy", "surface", "level")}
@@ -129,6 +180,6 @@ def test_step_parity(name, gpu):
     assert len(s1_on["pos"]) == len(exp["pos"]), "particle count after split/merge"
     check_equal("levels", s1_on["level"], exp["level"])
     for k in ("pos", "vel", "ev", "acc", "energy"):
-        check_close(f"adapted {k}", s1_on[k], exp[k])
+        check_close(f"{name}/adapted {k}", s1_on[k], exp[k])
     for k in ("dens", "press", "surface"):
-        check_close(f"adapted {k}", s1_on[k], exp[k])
+        check_close(f"{name}/adapted {k}", s1_on[k], exp[k])

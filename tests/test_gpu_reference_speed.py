@@ -1,12 +1,17 @@
-"""Speed against the reference itself, on the reference's own scene.
+"""Speed against the reference itself, on the reference's own scenes.
 
-The unmodified reference (oracle/_ref/libref_3d2_gpu.so, compiled from its
-sources for sm_100a) steps its default SPH-3D-2 scene with split and merge
-on: each animation() ends with the synchronous readback of every particle.
-The same scene and constants through this library's C-ABI, with the same
-per-step readback into page-locked host memory, must be faster.  Both times
-are host wall-clock per step (the reference is synchronous by construction).
-Prints one JSON line with the numbers and this library's stage times.
+The unmodified reference (oracle/_ref/libref_<v>_gpu.so, compiled from its
+sources for sm_100a) steps the scene its app starts with, split and merge
+on, in each of its three solvers:
+  2d   SPH-2D add_init_particle   (SPH-2D/sph_system.cpp:148-162, sph_main.cpp:45)
+  3d2  SPH-3D-2 add_box_particle  (SPH-3D-2/sph_system.cpp:247-264)
+  3d4  SPH-3D-4 add_box_particle  (SPH-3D-4/sph_system.cpp:248-289, sph_main.cpp:341)
+Each animation()/animate() ends with the synchronous readback of every
+particle.  The same scene and constants through this library's C-ABI, with
+the same per-step readback into page-locked host memory, must be faster.
+Both times are host wall-clock per step (the reference is synchronous by
+construction).  Prints one JSON line per solver with the numbers and this
+library's stage times.
 """
 import ctypes as C
 import json
@@ -24,8 +29,13 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 STEPS = 40
 
 
-def _reference_ms_per_step():
-    path = os.path.join(ROOT, "oracle", "_ref", "libref_3d2_gpu.so")
+VARIANTS = {"2d": (sph.PRESET_REF_2D, scenes.ref_init_2d, "SPH-2D add_init_particle"),
+            "3d2": (sph.PRESET_REF_3D2, scenes.ref_box_3d2, "SPH-3D-2 add_box_particle"),
+            "3d4": (sph.PRESET_REF_3D4, scenes.ref_box_3d4, "SPH-3D-4 add_box_particle")}
+
+
+def _reference_ms_per_step(v):
+    path = os.path.join(ROOT, "oracle", "_ref", f"libref_{v}_gpu.so")
     if not os.path.exists(path):
         return None, None
     lib = C.CDLL(path)
@@ -49,11 +59,12 @@ def _reference_ms_per_step():
     return dt * 1e3, int(lib.ref_num_particles(h))
 
 
-def _ours_ms_per_step(graph):
+def _ours_ms_per_step(v, graph):
     import torch
-    cfg = sph.preset(sph.PRESET_REF_3D2)
+    preset, scene, _ = VARIANTS[v]
+    cfg = sph.preset(preset)
     cfg.use_split = cfg.use_merge = 1
-    pos, vel, lvl = scenes.ref_box_3d2(cfg)
+    pos, vel, lvl = scene(cfg)
     s = sph.Solver(cfg)
     s.set_graph(graph)
     s.set_state(dict(pos=pos, vel=vel, level=lvl))
@@ -73,11 +84,12 @@ def _ours_ms_per_step(graph):
     return dt * 1e3, n, stages
 
 
-def test_faster_than_reference_on_its_own_scene(gpu):
-    ref_ms, ref_n = _reference_ms_per_step()
-    ours_ms, n, stages = _ours_ms_per_step(False)
-    graph_ms, _, _ = _ours_ms_per_step(True)
-    print(json.dumps({"scene": "SPH-3D-2 default, split+merge, readback every step", "steps": STEPS,
+@pytest.mark.parametrize("v", list(VARIANTS))
+def test_faster_than_reference_on_its_own_scene(v, gpu):
+    ref_ms, ref_n = _reference_ms_per_step(v)
+    ours_ms, n, stages = _ours_ms_per_step(v, False)
+    graph_ms, _, _ = _ours_ms_per_step(v, True)
+    print(json.dumps({"scene": f"{VARIANTS[v][2]}, split+merge, readback every step", "steps": STEPS,
                       "reference_ms_per_step": ref_ms, "reference_particles": ref_n,
                       "ours_ms_per_step": ours_ms, "ours_graph_ms_per_step": graph_ms, "ours_particles": n,
                       "ours_stages_ms": {k: round(v, 4) for k, v in stages}}))

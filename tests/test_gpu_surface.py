@@ -3,6 +3,12 @@
 * The grid the step builds (grid_every = 1, the reference's display mode 2)
   from the reference's own state S0 is compared with the reference's grid
   (tests/golden) and with the FP64 oracle.
+* The config-mode surface the SI presets build (kernel-length splat,
+  vertices interpolated at the iso value 0.5 rho0) is compared with the FP64
+  oracle: the grid with the oracle's splat, and the mesh with the oracle's
+  marching cubes (oracle/mc.py) on the same FP32 grid (cube cases and
+  triangle counts bit-exact, vertices and normals within 1e-5), on an SI
+  block and on a crop of the 1.1M-particle benchmark workload.
 * Marching cubes on the reference's exact grid (sph_surface_from_grid) is
   compared with the reference's own CPU marching cubes on the same grid:
   same triangle count, same triangles per cube in the same cube order, the
@@ -36,7 +42,7 @@ def _cfg(v, grid):
 
 def _mesh(solver, fn, *args):
     G = int(np.prod([solver.cfg.ndens[a] for a in range(3)]))
-    mx = 3 * G
+    mx = min(3 * G, int(solver.cfg.max_triangles)) if solver.cfg.max_triangles else 3 * G
     bufs = [np.zeros((mx, 3), np.float32) for _ in range(6)]
     mv = sph.MeshView()
     mv.max_triangles = mx
@@ -156,3 +162,84 @@ def test_in_step_surface_on_si_block(gpu):
     v = mesh[:, :3].reshape(-1, 3)
     assert np.isfinite(v).all()
     assert (v >= 0).all() and (v <= np.array(list(cfg.world))).all()
+
+
+def _crop_x(scene, xmax):
+    pos, vel, lvl = scene
+    m = pos[:, 0] < xmax
+    return pos[m], vel[m], lvl[m]
+
+
+SI_SURFACES = {
+    # 24 x 24 x 12 block at s = 0.01 (two-way preset, 257 x 129 x 129 nodes)
+    "dam_3d2_block": (sph.PRESET_DAM_3D2, lambda c: scenes_mod().block_3d(c, (24, 24, 12), 0.01, seed=1)),
+    # the 1.1M-particle workload cut at x < 0.16 (262,144 particles; the full
+    # 257 x 257 x 129 node grid of the benchmark)
+    "dam_3d4_crop": (sph.PRESET_DAM_3D4, lambda c: _crop_x(scenes_mod().dam_3d4(c, seed=0), 0.16)),
+}
+
+
+def scenes_mod():
+    from sca2012_b200 import scenes
+    return scenes
+
+
+@pytest.mark.parametrize("name", list(SI_SURFACES))
+def test_si_surface_matches_oracle(name, gpu):
+    from oracle import mc as M
+    preset, scene = SI_SURFACES[name]
+    cfg = sph.preset(preset)
+    pos, vel, lvl = scene(cfg)
+    cfg.use_split = cfg.use_merge = 0
+    cfg.grid_every = 1
+    cfg.max_particle = 2 * len(pos)
+    assert cfg.mc_interpolate == 1 and cfg.splat_with_kernel == 1
+    s = sph.Solver(cfg)
+    s.set_state(dict(pos=pos, vel=vel, level=lvl))
+    s.step(2)
+    assert s.sync_status() == 0
+    s0 = s.get_state()
+    s.set_state(s0)
+    s.step(1)
+    assert s.sync_status() == 0
+    G = int(np.prod([cfg.ndens[a] for a in range(3)]))
+    dens = np.zeros(G, np.float32)
+    nrm = np.zeros((G, 3), np.float32)
+    assert s._lib.sph_density_grid(s._h, dens.ctypes.data_as(C.POINTER(C.c_float)),
+                                   nrm.ctypes.data_as(C.POINTER(C.c_float))) == 0
+    mesh = _mesh(s, s._lib.sph_extract_surface)
+    st = s.get_state()
+    s.close()
+
+    # (1) the kernel-length splat on the stale cells with the new positions
+    key, idx, cs, ce = O.sort(cfg, s0["pos"])
+    d64, n64 = O.density_grid(cfg, st["pos"], s0["level"], idx, cs, ce)
+    check_close(f"{name}/grid density vs oracle", dens, d64)
+
+    # (2) marching cubes on the GPU's own grid: same cases, same triangles in
+    # the same order, vertices interpolated at the iso value within 1e-5
+    tris, per_cube = M.marching_cubes(cfg, dens, nrm)
+    assert len(mesh) == len(tris), (len(mesh), len(tris))
+    assert len(mesh) > 1000
+    check_close(f"{name}/mesh vertices", mesh[:, :3].reshape(-1, 3), tris[:, :3].reshape(-1, 3))
+    np.testing.assert_allclose(mesh[:, 3:].reshape(-1, 3), tris[:, 3:].reshape(-1, 3), rtol=0, atol=1e-6)
+
+    # (3) cube cases from the FP32 grid against those of the FP64 grid: every
+    # cube that differs has a corner node within 1e-5 of the iso value
+    c32 = M.cube_cases(cfg, dens)
+    c64 = M.cube_cases(cfg, d64)
+    diff = np.flatnonzero(c32 != c64)
+    if len(diff):
+        R, Cn, L = (int(cfg.ndens[a]) for a in range(3))
+        near = np.abs(d64 - float(cfg.iso_value)) <= 1e-5 * float(cfg.iso_value)
+        near3 = near.reshape(L, Cn, R).transpose(2, 1, 0)
+        qx = diff // ((Cn - 1) * (L - 1))
+        qy = (diff // (L - 1)) % (Cn - 1)
+        qz = diff % (L - 1)
+        amb = np.zeros(len(diff), bool)
+        for ox in (0, 1):
+            for oy in (0, 1):
+                for oz in (0, 1):
+                    amb |= near3[qx + ox, qy + oy, qz + oz]
+        assert amb.all(), f"{int((~amb).sum())} cubes differ away from the iso value"
+    print(f"{name}: {len(mesh)} triangles, {len(diff)} of {len(c32)} cube cases at an ambiguous node")
