@@ -484,7 +484,8 @@ def run_ours(args, rank, world, local_rank):
 def small_configs(args):
     """The 2D plain dam break (4,096 particles, no adaptivity, 1,000-step
     config) and the 3D two-way dam break (131,072 particles, 500-step config)
-    on the GPU, eager and CUDA-graph, 200 timed steps each; and the FP64
+    on the GPU, eager, CUDA-graph and persistent (one cooperative launch per
+    step), 200 timed steps each; and the FP64
     oracle on the host, one thread and all threads, a few steps of each of
     the three workloads (particle-steps/s)."""
     import torch
@@ -497,9 +498,10 @@ def small_configs(args):
         cfg = sph.preset(pre)
         cfg.use_split = cfg.use_merge = adapt
         pos, vel, lvl = make(cfg, seed=args.seed)
-        for mode in ("eager", "graph"):
+        for mode in ("eager", "graph", "persistent"):
             s = sph.Solver(cfg)
             s.set_graph(mode == "graph")
+            s.set_persistent(mode == "persistent")
             s.set_state(dict(pos=pos, vel=vel, level=lvl))
             s.step(5)
             st = torch.cuda.ExternalStream(s.stream_ptr)

@@ -50,6 +50,7 @@ extern "C" {
 #define SPH_ERR_NO_DEVICE  4  /* no CUDA device / kernels not loadable */
 #define SPH_ERR_NONFINITE  5  /* non-finite position detected by the step */
 #define SPH_ERR_RANGE      6  /* size beyond a fixed maximum of the entry point */
+#define SPH_ERR_TIMEOUT    7  /* a grid-wide barrier of the persistent step gave up waiting */
 
 /* ---- presets (sph_config_preset) ---- */
 #define SPH_PRESET_REF_2D    0  /* SPH-2D/sph_system.cpp:5-146            */
@@ -235,6 +236,22 @@ int sph_set_scenes(sph_handle *h, uint32_t nscenes, const sph_scene *scenes);
  * build the density grid and surface run uncaptured.  Same results, fewer
  * launch overheads for small particle counts. */
 int sph_set_graph(sph_handle *h, int on);
+
+/* on != 0: sph_step runs each step as ONE cooperative launch (the stages
+ * separated by grid-wide barriers instead of launch boundaries), for scenes
+ * small enough that launches and the drain between them, not the work, set
+ * the step time.  Results are bit for bit those of the ordinary launches;
+ * steps that build the density grid and surface, and profiled steps, use
+ * the ordinary launches.  Takes precedence over sph_set_graph.  No
+ * counterpart in the reference, which launches every stage separately
+ * (SPH-3D-2/sph_system.cpp:302-404).
+ * spin_limit: how many times a block polls a barrier before it gives up
+ * (SPH_PERSISTENT_SPIN_DEFAULT: about a second; 0: at the first poll).  A
+ * block that gives up ends the launch with SPH_ERR_TIMEOUT (reported by
+ * sph_sync); that step writes no state, later steps do nothing until the
+ * state is restored with sph_set_state, and the handle stays usable. */
+#define SPH_PERSISTENT_SPIN_DEFAULT (1u << 22)
+int sph_set_persistent(sph_handle *h, int on, uint32_t spin_limit);
 
 /* Synchronises and returns the device-side status (capacity / non-finite). */
 int sph_sync(sph_handle *h);

@@ -14,7 +14,7 @@ import numpy as np
 from . import _abi
 from ._abi import Config, StateView, DebugView, MeshView  # noqa: F401
 from ._abi import (SPH_OK, SPH_ERR_INVALID, SPH_ERR_CAPACITY, SPH_ERR_CUDA, SPH_ERR_NO_DEVICE,  # noqa: F401
-                   SPH_ERR_NONFINITE, SPH_ERR_RANGE)
+                   SPH_ERR_NONFINITE, SPH_ERR_RANGE, SPH_ERR_TIMEOUT)
 from ._abi import (PRESET_REF_2D, PRESET_REF_3D2, PRESET_REF_3D4, PRESET_DAM_2D,  # noqa: F401
                    PRESET_DAM_3D2, PRESET_DAM_3D4, PRESET_ROLLOUT_3D)
 
@@ -106,6 +106,11 @@ class Solver:
     def set_graph(self, on=True):
         """Replay steps as captured CUDA graphs (same results, fewer launches)."""
         self._check(self._lib.sph_set_graph(self._h, 1 if on else 0), "sph_set_graph")
+
+    def set_persistent(self, on=True, spin_limit=_abi.PERSISTENT_SPIN_DEFAULT):
+        """Run each step as one cooperative launch (same results as the
+        ordinary launches); spin_limit bounds every barrier wait."""
+        self._check(self._lib.sph_set_persistent(self._h, 1 if on else 0, int(spin_limit)), "sph_set_persistent")
 
     def set_scenes(self, boxes):
         """Batched scenes: boxes is a list of (lo, hi, viscosity, gas_constant)

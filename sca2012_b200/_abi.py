@@ -13,6 +13,8 @@ SPH_ERR_CUDA = 3
 SPH_ERR_NO_DEVICE = 4
 SPH_ERR_NONFINITE = 5
 SPH_ERR_RANGE = 6
+SPH_ERR_TIMEOUT = 7
+PERSISTENT_SPIN_DEFAULT = 1 << 22
 
 PRESET_REF_2D = 0
 PRESET_REF_3D2 = 1
@@ -139,6 +141,7 @@ SIGNATURES = [
     ("sph_step", C.c_int, [H, C.c_int]),
     ("sph_set_scenes", C.c_int, [H, C.c_uint32, C.POINTER(Scene)]),
     ("sph_set_graph", C.c_int, [H, C.c_int]),
+    ("sph_set_persistent", C.c_int, [H, C.c_int, C.c_uint32]),
     ("sph_sync", C.c_int, [H]),
     ("sph_get_num_particles", C.c_int, [H, UP]),
     ("sph_get_state", C.c_int, [H, C.POINTER(StateView)]),

@@ -11,6 +11,7 @@
 #include "sph_kernels.cuh"
 #include "sph_scan.cuh"
 #include "sph_mc.cuh"
+#include "sph_persistent.cuh"
 
 #include <cuda_runtime.h>
 #include <algorithm>
@@ -80,6 +81,11 @@ struct sph_handle {
     uint32_t tune_bs[SPH_TUNE_STAGES] = {256, 256, 256, 256, 256, 256, 256, 256};
     uint32_t tune_bpsm[SPH_TUNE_STAGES] = {8, 8, 8, 8, 8, 8, 8, 8};
     uint32_t tune_minb[SPH_TUNE_STAGES] = {0, 0, 0, 0, 0, 1, 0, 0};   // 1: register-capped variant
+    // persistent step: the whole step as one cooperative launch
+    bool persistent = false;
+    uint32_t spin_limit = SPH_PERSISTENT_SPIN_DEFAULT;
+    GridSync *gsync = nullptr;
+    int persist_blocks_per_sm[2] = {0, 0};   // resident blocks of k_step_persistent<2|3> (0: not queried)
 };
 
 namespace {
@@ -285,6 +291,56 @@ template <int DIM> int run_step(sph_handle *h)
     return cuda_check(h, "sph_step launch");
 }
 
+// The step as one cooperative launch of k_step_persistent (sph_persistent.cuh):
+// same stages, same arithmetic, grid-wide barriers instead of launch
+// boundaries.  The grid holds one block of 256 threads per 256 particles of
+// the live-count bound, at most what fits resident on the device.
+constexpr int kPersistThreads = 256;
+
+template <int DIM> int run_step_persistent(sph_handle *h)
+{
+    const sph_config &c = h->cfg;
+    const int p = h->cur;
+    Counters *cin = h->cnt + p, *cout = h->cnt + (p ^ 1);
+    CanonPtrs in = h->buf[p], out = h->buf[p ^ 1];
+    h->w.pos_comp = c.compensated_positions ? 1u : 0u;
+    WorkPtrs w = h->w;
+    if (c.walk_only) w.nlist = w.ncnt = nullptr;
+    auto kern = k_step_persistent<DIM, kPersistThreads>;
+    int &per_sm = h->persist_blocks_per_sm[DIM - 2];
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPersistThreads, 0) != cudaSuccess ||
+            per_sm < 1) {
+            per_sm = 0;
+            return cuda_check(h, "persistent step occupancy");
+        }
+    }
+    const uint32_t want = std::max<uint32_t>(1u, (h->n_ub + kPersistThreads - 1) / kPersistThreads);
+    const uint32_t G = std::min<uint32_t>({want, (uint32_t)(per_sm * h->num_sms), (uint32_t)kScanBlocks});
+    PersistArgs a;
+    a.gs = h->gsync;
+    a.spin_limit = h->spin_limit;
+    a.ncells = h->ncells;
+    a.cap = h->cap;
+    a.scan_blocks = h->scan_blocks;
+    a.scan_grand = h->scan_grand;
+    a.want_tv = h->debug ? 1 : 0;
+    a.ranks = (c.use_split || c.use_merge) ? 1 : 0;
+    sph_config cc = c;
+    void *args[] = {&cc, &cin, &cout, &in, &out, &w, &a};
+    cudaMemsetAsync(h->gsync, 0, sizeof(GridSync), h->stream);
+    if (cudaLaunchCooperativeKernel((void *)kern, dim3(G), dim3(kPersistThreads), args, 0, h->stream) !=
+        cudaSuccess)
+        return cuda_check(h, "persistent step launch");
+    h->last_launches += 1;
+    h->cur = p ^ 1;
+    h->step_index++;
+    uint64_t ub = h->n_ub;
+    if (c.use_split) ub *= (c.split_ways == 4 ? 4u : 2u);
+    h->n_ub = (uint32_t)std::min<uint64_t>(ub, h->cap);
+    return cuda_check(h, "sph_step persistent");
+}
+
 void pack4(const float *src, int dim, uint32_t n, std::vector<float4> &dst, const uint32_t *level)
 {
     dst.resize(n);
@@ -325,6 +381,7 @@ void write_n(sph_handle *h, uint32_t n)
     cudaMemcpyAsync(&c0, &h->cnt[h->cur], sizeof(Counters), cudaMemcpyDeviceToHost, h->stream);
     cudaStreamSynchronize(h->stream);
     c0.n = n;
+    c0.error &= ~(1u << SPH_ERR_TIMEOUT);   // a new state: steps may run again after a timeout
     cudaMemcpyAsync(&h->cnt[h->cur], &c0, sizeof(Counters), cudaMemcpyHostToDevice, h->stream);
     cudaStreamSynchronize(h->stream);
 }
@@ -400,6 +457,7 @@ int sph_create(const sph_config *cfg, sph_handle **out)
     rc |= dalloc(h, &w.macc, cap); rc |= dalloc(h, &w.menergy, cap);
     rc |= dalloc(h, &h->scan_blocks, (size_t)kScanBlocks * 2);
     rc |= dalloc(h, &h->scan_grand, 4);
+    rc |= dalloc(h, &h->gsync, 1);
     if (!rc) rc = mc_alloc(h->mc, *cfg, h->allocs);
     if (rc) {
         fprintf(stderr, "sph_create: %s\n", h->err.c_str());
@@ -600,7 +658,9 @@ int sph_step(sph_handle *h, int nsteps)
         const bool surface_due = h->cfg.dim == 3 && h->cfg.grid_every && h->mc.nodes &&
                                  h->step_index % h->cfg.grid_every == 0;
         int rc;
-        if (h->use_graph && !h->profiling && !surface_due) {
+        if (h->persistent && !h->profiling && !surface_due) {
+            rc = h->cfg.dim == 3 ? run_step_persistent<3>(h) : run_step_persistent<2>(h);
+        } else if (h->use_graph && !h->profiling && !surface_due) {
             const int p = h->cur;
             if (!h->graph[p] || h->graph_grid[p] != launch_key(h)) {
                 rc = capture_step(h);
@@ -621,6 +681,14 @@ int sph_step(sph_handle *h, int nsteps)
         if (rc) return rc;
         h->have_step = true;
     }
+    return SPH_OK;
+}
+
+int sph_set_persistent(sph_handle *h, int on, uint32_t spin_limit)
+{
+    if (!h) return SPH_ERR_INVALID;
+    h->persistent = on != 0;
+    h->spin_limit = spin_limit;
     return SPH_OK;
 }
 
@@ -712,6 +780,8 @@ int sph_sync(sph_handle *h)
             if (err & (1u << code)) {
                 h->err = code == SPH_ERR_CAPACITY    ? "particle capacity exceeded by a split (splits skipped)"
                          : code == SPH_ERR_NONFINITE ? "a particle's position or velocity became non-finite"
+                         : code == SPH_ERR_TIMEOUT   ? "a barrier of the persistent step gave up waiting; "
+                                                       "restore the state with sph_set_state"
                                                      : "device reported an error";
                 return code;
             }

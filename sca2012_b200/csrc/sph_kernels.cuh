@@ -22,7 +22,11 @@
 // Every decision that is an integer outcome of float arithmetic (cell keys,
 // r^2 < h^2, h - r > 0, the split/merge scores) is evaluated with explicit
 // round-to-nearest intrinsics in a fixed order, so the CPU oracle's FP32
-// replica reproduces it bit for bit.
+// replica reproduces it bit for bit.  Every sum with a product operand in the
+// step's bodies is written as an explicit __fmaf_rn / __fadd_rn too: the
+// compiler then has no multiply-add to contract, so a body compiled into a
+// standalone kernel and into the persistent step kernel (sph_persistent.cuh)
+// rounds the same way and the two give the same bits.
 #pragma once
 #include <cstdint>
 #include "../../include/sph/sph.h"
@@ -183,9 +187,19 @@ __device__ __forceinline__ float split_score(const sph_config &c, float e, float
 __device__ __forceinline__ uint32_t grid_stride_start() { return blockIdx.x * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ uint32_t grid_stride() { return gridDim.x * blockDim.x; }
 
+// A load of data the kernel does not write.  NC = true takes the read-only
+// (non-coherent) data path; the persistent step kernel (sph_persistent.cuh)
+// passes NC = false, because inside its single launch a later stage reads
+// what an earlier stage wrote.
+template <bool NC, class T> __device__ __forceinline__ T ldro(const T *p)
+{
+    if constexpr (NC) return __ldg(p);
+    else return *p;
+}
+
 // Row ranges of the 3^DIM neighbourhood of cell q: rows (dy, dz); each row is
 // the slot range [off[key(x0)], off[key(x1)+1]) of cells x0..x1.
-template <int DIM>
+template <int DIM, bool NC = true>
 __device__ __forceinline__ int row_range(const sph_config &c, const uint32_t *__restrict__ off, uint3 q,
                                          int dy, int dz, uint32_t &b, uint32_t &e)
 {
@@ -196,15 +210,15 @@ __device__ __forceinline__ int row_range(const sph_config &c, const uint32_t *__
     uint32_t x1 = q.x + 1 < c.ncell[0] ? q.x + 1 : q.x;
     uint32_t k0 = key_of(c, x0, (uint32_t)y, (uint32_t)z);
     uint32_t k1 = key_of(c, x1, (uint32_t)y, (uint32_t)z);
-    b = __ldg(off + k0);
-    e = __ldg(off + k1 + 1);
+    b = ldro<NC>(off + k0);
+    e = ldro<NC>(off + k1 + 1);
     return 1;
 }
 
 // ------------------------------------------------------------ 1. hash
-template <int DIM, int BS = kThreads>
-__global__ void __launch_bounds__(BS) k_hash(sph_config c, const Counters *__restrict__ cnt,
-                                                  CanonPtrs st, WorkPtrs w)
+template <int DIM>
+__device__ __forceinline__ void hash_body(const sph_config &c, const Counters *cnt, const CanonPtrs &st,
+                                          const WorkPtrs &w)
 {
     const uint32_t n = cnt->n;
     for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) {
@@ -222,13 +236,26 @@ __global__ void __launch_bounds__(BS) k_hash(sph_config c, const Counters *__res
     }
 }
 
+template <int DIM, int BS = kThreads>
+__global__ void __launch_bounds__(BS) k_hash(sph_config c, const Counters *__restrict__ cnt,
+                                                  CanonPtrs st, WorkPtrs w)
+{
+    hash_body<DIM>(c, cnt, st, w);
+}
+
 // ------------------------------------------------------------ 3. scatter
-template <int BS = kThreads>
-__global__ void __launch_bounds__(BS) k_scatter(const Counters *__restrict__ cnt, WorkPtrs w)
+template <bool NC>
+__device__ __forceinline__ void scatter_body(const Counters *cnt, const WorkPtrs &w)
 {
     const uint32_t n = cnt->n;
     for (uint32_t i = grid_stride_start(); i < n; i += grid_stride())
-        w.tmp[__ldg(w.cell_off + w.key[i]) + w.slot[i]] = i;
+        w.tmp[ldro<NC>(w.cell_off + w.key[i]) + w.slot[i]] = i;
+}
+
+template <int BS = kThreads>
+__global__ void __launch_bounds__(BS) k_scatter(const Counters *__restrict__ cnt, WorkPtrs w)
+{
+    scatter_body<true>(cnt, w);
 }
 
 // ------------------------------------------------------------ 4. stable order + gather
@@ -236,14 +263,14 @@ __global__ void __launch_bounds__(BS) k_scatter(const Counters *__restrict__ cnt
 // keys in ascending particle index, as thrust's radix sort_by_key leaves
 // them, SPH-3D-2/sph_system.cu:119-129) is restored by ranking each particle
 // among its cell's members.  Then the state is gathered into key order.
-template <int BS = kThreads>
-__global__ void __launch_bounds__(BS) k_reorder(const Counters *__restrict__ cnt, CanonPtrs st, WorkPtrs w)
+template <bool NC>
+__device__ __forceinline__ void reorder_body(const Counters *cnt, const CanonPtrs &st, const WorkPtrs &w)
 {
     const uint32_t n = cnt->n;
     for (uint32_t s = grid_stride_start(); s < n; s += grid_stride()) {
         uint32_t i = w.tmp[s];
         uint32_t k = w.key[i];
-        uint32_t b = __ldg(w.cell_off + k), e = __ldg(w.cell_off + k + 1);
+        uint32_t b = ldro<NC>(w.cell_off + k), e = ldro<NC>(w.cell_off + k + 1);
         uint32_t r = 0;
         for (uint32_t t = b; t < e; ++t) r += w.tmp[t] < i;
         uint32_t d = b + r;
@@ -256,6 +283,12 @@ __global__ void __launch_bounds__(BS) k_reorder(const Counters *__restrict__ cnt
         if (w.nscenes) w.sscene[d] = st.scene[i];
         if (w.pos_comp) w.spos_lo[d] = st.pos_lo[i];
     }
+}
+
+template <int BS = kThreads>
+__global__ void __launch_bounds__(BS) k_reorder(const Counters *__restrict__ cnt, CanonPtrs st, WorkPtrs w)
+{
+    reorder_body<true>(cnt, st, w);
 }
 
 // ------------------------------------------------------------ warp-lockstep pair loop
@@ -291,7 +324,7 @@ struct WarpPairSmem {
 // the lane's list read slot `self`), for callers whose fetched data fits in
 // registers.  Every lane of the warp must call it (active = false for a lane
 // without a particle).
-template <int DIM, int AHEAD = 0, class Accept, class Pair>
+template <int DIM, int AHEAD = 0, bool NC = true, class Accept, class Pair>
 __device__ __forceinline__ void warp_pairs(const sph_config &c, const uint32_t *__restrict__ off,
                                            const float4 *__restrict__ pos, bool active, uint3 q,
                                            WarpPairSmem &sm, Accept accept, Pair pair, uint32_t self = 0)
@@ -305,7 +338,7 @@ __device__ __forceinline__ void warp_pairs(const sph_config &c, const uint32_t *
         while (++row < nrows) {
             const int dy = row % 3 - 1, dz = DIM == 3 ? row / 3 - 1 : 0;
             uint32_t b, ee;
-            if (row_range<DIM>(c, off, q, dy, dz, b, ee) && ee > b) {
+            if (row_range<DIM, NC>(c, off, q, dy, dz, b, ee) && ee > b) {
                 t = b;
                 e = ee;
                 return true;
@@ -356,8 +389,11 @@ __device__ __forceinline__ void warp_pairs(const sph_config &c, const uint32_t *
 // ------------------------------------------------------------ 5. density
 // rho_i = m_i poly6_i h_i^6 + sum_{j != i, skip <= r^2 < h_i^2} m_j poly6_i (h_i^2 - r^2)^3
 // p_i = k ((rho_i / rho0)^3 - 1)         (SPH-3D-2/sph_system.cu:338-677)
-template <int DIM, int BS = kThreads>
-__global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restrict__ cnt, WorkPtrs w)
+#ifndef SPH_DENS_MINB
+#define SPH_DENS_MINB 1
+#endif
+template <int DIM, bool NC>
+__device__ __forceinline__ void density_body(const sph_config &c, Counters *cnt, const WorkPtrs &w)
 {
     const uint32_t n = cnt->n;
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt->disp2_max = 0u;   // the force pass takes the max
@@ -386,12 +422,28 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restri
         // fits 32 bits under the lists' 12 GB allocation limit)
         uint32_t *const lbase = rec ? w.nlist + (size_t)s * 4u : nullptr;
         const uint32_t row4 = w.nl_stride * 4u;
+#ifdef SPH_DENS_F2
+        const float2 npi = make_float2(-pi.x, -pi.y);
+#endif
         auto add = [&](uint32_t t, float4 pj) {   // t != s (the walk skips s)
+#ifdef SPH_DENS_F2
+            const float2 dxy = __fadd2_rn(make_float2(pj.x, pj.y), npi);
+            float r2 = __fmaf_rn(dxy.x, dxy.x, __fmul_rn(dxy.y, dxy.y));
+            if (DIM == 3) {
+                const float dzz = __fsub_rn(pj.z, pi.z);
+                r2 = __fmaf_rn(dzz, dzz, r2);
+            }
+#else
             float dx, dyy, dzz;
             const float r2 = r2_of<DIM>(pj, pi, dx, dyy, dzz);
+#endif
+#ifdef SPH_DENS_NOSKIP
+            if (r2 < h2) {
+#else
             if (!(r2 < skip) && r2 < h2) {
+#endif
                 const float x = h2 - r2;
-                rho += (pj.w == 1.0f ? mp0 : mp1) * (x * x * x);
+                rho = __fmaf_rn(pj.w == 1.0f ? mp0 : mp1, x * x * x, rho);
                 ++nb;
             }
             if (rec && r2 < re2) {
@@ -402,21 +454,21 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restri
         auto range = [&](uint32_t b, uint32_t e) {
             uint32_t t = b;
             for (; t + 4 <= e; t += 4) {
-                const float4 p0 = __ldg(w.spos + t), p1 = __ldg(w.spos + t + 1), p2 = __ldg(w.spos + t + 2),
-                             p3 = __ldg(w.spos + t + 3);
+                const float4 p0 = ldro<NC>(w.spos + t), p1 = ldro<NC>(w.spos + t + 1),
+                             p2 = ldro<NC>(w.spos + t + 2), p3 = ldro<NC>(w.spos + t + 3);
                 add(t, p0);
                 add(t + 1, p1);
                 add(t + 2, p2);
                 add(t + 3, p3);
             }
-            for (; t < e; ++t) add(t, __ldg(w.spos + t));
+            for (; t < e; ++t) add(t, ldro<NC>(w.spos + t));
         };
 #pragma unroll 1
         for (int dz = (DIM == 3 ? -1 : 0); dz <= (DIM == 3 ? 1 : 0); ++dz)
 #pragma unroll 1
             for (int dy = -1; dy <= 1; ++dy) {
                 uint32_t b, e;
-                if (!row_range<DIM>(c, w.cell_off, q, dy, dz, b, e)) continue;
+                if (!row_range<DIM, NC>(c, w.cell_off, q, dy, dz, b, e)) continue;
                 if (dy == 0 && dz == 0) {   // the particle's own row: around its slot
                     range(b, s);
                     range(s + 1u, e);
@@ -424,10 +476,10 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restri
                     range(b, e);
                 }
             }
-        rho += c.mass[li] * poly6 * c.kernel6[li];   // self term
+        rho = __fadd_rn(rho, c.mass[li] * poly6 * c.kernel6[li]);   // self term
         float r = rho / c.rest_density;
         const float gas = w.nscenes ? w.scene_tab[2 * min(w.sscene[s], w.nscenes - 1u) + 1].w : c.gas_constant;
-        float p = (r * r * r - 1.0f) * gas;
+        float p = __fsub_rn(r * r * r, 1.0f) * gas;
         const float pr2 = p / (rho * rho), mr = c.mass[li] / rho;
         w.saux[s] = make_float4(rho, p, pr2, mr);
         const float4 evs = w.sev[s];
@@ -438,16 +490,21 @@ __global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restri
     }
 }
 
+template <int DIM, int BS = kThreads>
+__global__ void __launch_bounds__(BS, SPH_DENS_MINB) k_density(sph_config c, Counters *__restrict__ cnt, WorkPtrs w)
+{
+    density_body<DIM, true>(c, cnt, w);
+}
+
 // ------------------------------------------------------------ 6. force + integrate
 // Pressure, viscosity and colour-field terms (SPH-3D-2/sph_system.cu:679-1137,
 // 2D SPH-2D/sph_system.cu:462-790), then the integrator and walls
 // (SPH-3D-2/sph_system.cu:204-322, SPH-2D/sph_system.cu:198-252).  The
 // integrated state goes to the *_n arrays so the loop never sees it.
-template <int DIM, int BS = kThreads, int MINB = 3>
-__global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Counters *__restrict__ cnt,
-                                                              WorkPtrs w)
+template <int DIM, int BS, bool NC>
+__device__ __forceinline__ void force_integrate_body(const sph_config &c, Counters *cnt, const WorkPtrs &w,
+                                                     WarpPairSmem *smem)
 {
-    __shared__ WarpPairSmem smem[BS / 32];
     const uint32_t n = cnt->n;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     // warp-uniform grid-stride loop: a warp takes 32 consecutive slots
@@ -474,7 +531,7 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
         q.z = DIM == 3 ? k / (c.ncell[0] * c.ncell[1]) : 0u;
         float fx = 0.f, fy = 0.f, fz = 0.f, gx = 0.f, gy = 0.f, gz = 0.f, lap = 0.f;
         if (DIM == 2)   // self term, SPH-2D/sph_system.cu:599-603 (0 with the integer 3/4)
-            lap += ilap * ai.w * hi2 * (0.0f - c.lapc_three_quarters * hi2);
+            lap = __fmaf_rn(ilap * ai.w * hi2, __fsub_rn(0.0f, c.lapc_three_quarters * hi2), lap);
         // pairs with r^2 < max(h_i^2, h_j^2) and r^2 >= close_r2 (:797-804)
         const float cut0 = fmaxf(hi2, c.kernel2[0]), cut1 = fmaxf(hi2, c.kernel2[1]);
         const float close = c.close_r2;
@@ -505,8 +562,8 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
                 ivk = ivis * ikr;
                 const float x = hi2 - r2;
                 const float tg = igrad * mrj * x * x;   // -grad_poly6 * m_j/rho_j * (h^2-r^2)^2
-                gx += tg * rx; gy += tg * ry; gz += tg * rz;
-                lap += ilap * mrj * x * (r2 - c.lapc_three_quarters * x);
+                gx = __fmaf_rn(tg, rx, gx); gy = __fmaf_rn(tg, ry, gy); gz = __fmaf_rn(tg, rz, gz);
+                lap = __fmaf_rn(ilap * mrj * x, __fsub_rn(r2, c.lapc_three_quarters * x), lap);
             }
             const float jkr = __fsub_rn(c.kernel[lj], r);
             if (jkr > 0.0f) {
@@ -515,11 +572,11 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
             }
             // 1/r from the approximate reciprocal square root of r^2 (the h - r
             // decisions above keep the IEEE square root)
-            const float tp = (lj ? mimj1 : mimj0) * (ai.z + a.w) * (ipk + jpk) * 0.5f * rsqrtf(r2);
-            const float tv = (ai.w * mrj) * visc * (ivk + jvk) * 0.5f;
-            fx += -rx * tp + (b.y - evi.x) * tv;
-            fy += -ry * tp + (b.z - evi.y) * tv;
-            if (DIM == 3) fz += -rz * tp + (b.w - evi.z) * tv;
+            const float tp = (lj ? mimj1 : mimj0) * __fadd_rn(ai.z, a.w) * __fadd_rn(ipk, jpk) * 0.5f * rsqrtf(r2);
+            const float tv = (ai.w * mrj) * visc * __fadd_rn(ivk, jvk) * 0.5f;
+            fx = __fmaf_rn(__fsub_rn(b.y, evi.x), tv, __fmaf_rn(-rx, tp, fx));
+            fy = __fmaf_rn(__fsub_rn(b.z, evi.y), tv, __fmaf_rn(-ry, tp, fy));
+            if (DIM == 3) fz = __fmaf_rn(__fsub_rn(b.w, evi.z), tv, __fmaf_rn(-rz, tp, fz));
         };
         // the walk's test for a list entry (a list never holds the particle itself)
         auto accept_ab = [&](const float4 &a, const float4 &b) {
@@ -561,20 +618,20 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
                     if (accept_ab(a, b)) pair_ab(a, b);
                 }
         } else {
-            warp_pairs<DIM>(c, w.cell_off, w.spos, valid, q, smem[wib], accept, pair);
+            warp_pairs<DIM, 0, NC>(c, w.cell_off, w.spos, valid, q, smem[wib], accept, pair);
         }
         if (!valid) continue;
         // surface tension switch (SPH-3D-2/sph_system.cu:1113-1136)
-        const float nrm = sqrtf(gx * gx + gy * gy + gz * gz);
+        const float nrm = sqrtf(__fmaf_rn(gz, gz, __fmaf_rn(gy, gy, __fmul_rn(gx, gx))));
         if (nrm > c.surface_threshold) {
             const float f = c.surface_coef * lap / nrm;
-            fx += f * gx; fy += f * gy; fz += f * gz;
+            fx = __fmaf_rn(f, gx, fx); fy = __fmaf_rn(f, gy, fy); fz = __fmaf_rn(f, gz, fz);
         }
         if (DIM == 2 && c.extern_force_on) {   // SPH-2D/sph_system.cu:781-789
             float xl = __fsub_rn(pi.x, c.extern_click[0]), yl = __fsub_rn(pi.y, c.extern_click[1]);
             if (__fmaf_rn(xl, xl, __fmul_rn(yl, yl)) <= __fmul_rn(c.extern_len, c.extern_len)) {
-                fx += c.extern_force[0] * c.extern_coe;
-                fy += c.extern_force[1] * c.extern_coe;
+                fx = __fmaf_rn(c.extern_force[0], c.extern_coe, fx);
+                fy = __fmaf_rn(c.extern_force[1], c.extern_coe, fy);
             }
         }
         w.ssurf[s] = nrm;
@@ -589,11 +646,11 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
         float rad;
         if (c.integrator == SPH_INTEGRATE_REF2D) {
             rad = c.radius[li] / 2.0f;
-            a.x = (a.x + c.gravity[0] * dt) / rho;
-            a.y = (a.y + c.gravity[1] * dt) / rho;
-            v.x += a.x * dt; v.y += a.y * dt;
+            a.x = __fmaf_rn(c.gravity[0], dt, a.x) / rho;
+            a.y = __fmaf_rn(c.gravity[1], dt, a.y) / rho;
+            v.x = __fmaf_rn(a.x, dt, v.x); v.y = __fmaf_rn(a.y, dt, v.y);
             ev.x = (ev.x + v.x) / 2.0f; ev.y = (ev.y + v.y) / 2.0f;
-            x.x += v.x * dt; x.y += v.y * dt;
+            x.x = __fmaf_rn(v.x, dt, x.x); x.y = __fmaf_rn(v.y, dt, x.y);
         } else {
             rad = c.radius[li];
             if (c.integrator == SPH_INTEGRATE_REF3D) {
@@ -607,9 +664,9 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
                 v.x += c.gravity[0] * dt / rho; v.y += c.gravity[1] * dt / rho; v.z += c.gravity[2] * dt / rho;
             } else {
                 const float im = 1.0f / mi;
-                v.x += (a.x * im + c.gravity[0]) * dt;
-                v.y += (a.y * im + c.gravity[1]) * dt;
-                v.z += (a.z * im + c.gravity[2]) * dt;
+                v.x = __fmaf_rn(__fmaf_rn(a.x, im, c.gravity[0]), dt, v.x);
+                v.y = __fmaf_rn(__fmaf_rn(a.y, im, c.gravity[1]), dt, v.y);
+                v.z = __fmaf_rn(__fmaf_rn(a.z, im, c.gravity[2]), dt, v.z);
             }
             if (w.pos_comp) {
                 lo = w.spos_lo[s];
@@ -617,22 +674,23 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
                 comp_add(x.y, lo.y, __fmul_rn(v.y, dt));
                 if (DIM == 3) comp_add(x.z, lo.z, __fmul_rn(v.z, dt));
             } else {
-                x.x += v.x * dt; x.y += v.y * dt; x.z += v.z * dt;
+                x.x = __fmaf_rn(v.x, dt, x.x); x.y = __fmaf_rn(v.y, dt, x.y); x.z = __fmaf_rn(v.z, dt, x.z);
             }
             if (DIM == 3 && c.use_cylinder) {   // SPH-3D-2/sph_system.cu:242-282
                 for (int qq = 0; qq < 3; ++qq) {
                     const sph_sphere S = c.sphere[qq];
                     float dxs = x.x - S.pos[0], dys = x.y - S.pos[1], dzs = x.z - S.pos[2];
-                    float dist = sqrtf(dxs * dxs + dys * dys + dzs * dzs);
+                    float dist = sqrtf(__fmaf_rn(dzs, dzs, __fmaf_rn(dys, dys, __fmul_rn(dxs, dxs))));
                     float R = S.radius + rad;
                     if (dist < R) {
                         float sx = dxs / dist * R, sy = dys / dist * R, sz = dzs / dist * R;
-                        float il = rsqrtf(sx * sx + sy * sy + sz * sz);
+                        float il = rsqrtf(__fmaf_rn(sz, sz, __fmaf_rn(sy, sy, __fmul_rn(sx, sx))));
                         float nx = sx * il, ny = sy * il, nz = sz * il;
                         x.x = S.pos[0] + sx; x.y = S.pos[1] + sy; x.z = S.pos[2] + sz;
                         lo = make_float4(0.f, 0.f, 0.f, 0.f);
-                        float vn = v.x * nx + v.y * ny + v.z * nz;
-                        v.x -= S.damping * vn * nx; v.y -= S.damping * vn * ny; v.z -= S.damping * vn * nz;
+                        float vn = __fmaf_rn(v.z, nz, __fmaf_rn(v.y, ny, __fmul_rn(v.x, nx)));
+                        const float dv = S.damping * vn;
+                        v.x = __fmaf_rn(-dv, nx, v.x); v.y = __fmaf_rn(-dv, ny, v.y); v.z = __fmaf_rn(-dv, nz, v.z);
                     }
                 }
             }
@@ -680,6 +738,14 @@ __global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Coun
     }
 }
 
+template <int DIM, int BS = kThreads, int MINB = 3>
+__global__ void __launch_bounds__(BS, MINB) k_force_integrate(sph_config c, Counters *__restrict__ cnt,
+                                                              WorkPtrs w)
+{
+    __shared__ WarpPairSmem smem[BS / 32];
+    force_integrate_body<DIM, BS, true>(c, cnt, w, smem);
+}
+
 // ------------------------------------------------------------ 7. energy + split decision
 // Wavelet energy on the STALE cell lists (built at step start) with the NEW
 // positions (SPH-3D-2/sph_system.cu:1169-1546), then the split decision
@@ -688,14 +754,13 @@ __device__ __forceinline__ float wavelet(float x, float amp)
 {
     // psi(x) = amp * (x^2/4 - 1) * EXP^(-x^2/8), EXP = 2.718281f (sigma = 2)
     const float x2 = x * x;
-    return amp * (x2 * 0.25f - 1.0f) * exp2f(-x2 * 0.125f * 1.44269476f);
+    return amp * __fsub_rn(x2 * 0.25f, 1.0f) * exp2f(-x2 * 0.125f * 1.44269476f);
 }
 
-template <int DIM, int BS = kThreads, int MINB = 3>
-__global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counters *__restrict__ cnt,
-                                                           CanonPtrs st, WorkPtrs w, int want_tv)
+template <int DIM, int BS, bool NC>
+__device__ __forceinline__ void energy_split_body(const sph_config &c, Counters *cnt, const CanonPtrs &st,
+                                                  const WorkPtrs &w, int want_tv, WarpPairSmem *smem)
 {
-    __shared__ WarpPairSmem smem[BS / 32];
     const uint32_t n = cnt->n;
     // 2/(PI^0.25 * sqrt(3 sigma)) with PI = 3.141592f, sigma = 2
     const float amp = 2.0f / (powf(3.141592f, 0.25f) * sqrtf(6.0f));
@@ -728,12 +793,12 @@ __global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counter
             float rx, ry, rz;
             r2_of<DIM>(pi, pj, rx, ry, rz);
             const float wx = wavelet(rx * ih, amp), wy = wavelet(ry * ih, amp);
-            tsx += wx; tsy += wy;
-            tvx += vj.x * wx * isq; tvy += vj.y * wy * isq;
+            tsx = __fadd_rn(tsx, wx); tsy = __fadd_rn(tsy, wy);
+            tvx = __fmaf_rn(vj.x * wx, isq, tvx); tvy = __fmaf_rn(vj.y * wy, isq, tvy);
             if (DIM == 3) {
                 const float wz = wavelet(rz * ih, amp);
-                tsz += wz;
-                tvz += vj.z * wz * isq;
+                tsz = __fadd_rn(tsz, wz);
+                tvz = __fmaf_rn(vj.z * wz, isq, tvz);
             }
         };
         // the density pass's candidates when the particle kept its cell and the
@@ -769,10 +834,10 @@ __global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counter
                     if (kk + u < ne && accept(tt[u], g[u].p)) use(g[u]);
             }
         }
-        warp_pairs<DIM, 4>(c, w.cell_off, w.spos_n, walk, q, smem[wib], accept, fetch_use(fetch, use), s);
+        warp_pairs<DIM, 4, NC>(c, w.cell_off, w.spos_n, walk, q, smem[wib], accept, fetch_use(fetch, use), s);
         if (!valid) continue;
         tvx /= tsx; tvy /= tsy; tvz = DIM == 3 ? tvz / tsz : 0.f;
-        float energy = 0.5f * (tvx * tvx + tvy * tvy);
+        float energy = 0.5f * __fmaf_rn(tvx, tvx, __fmul_rn(tvy, tvy));
         if (c.energy_mass_weight) energy *= c.mass[li];
         w.senergy[s] = energy;
         if (want_tv) w.stv[s] = make_float4(tvx, tvy, tvz, 0.f);
@@ -797,10 +862,18 @@ __global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counter
     }
 }
 
+template <int DIM, int BS = kThreads, int MINB = 3>
+__global__ void __launch_bounds__(BS, MINB) k_energy_split(sph_config c, Counters *__restrict__ cnt,
+                                                           CanonPtrs st, WorkPtrs w, int want_tv)
+{
+    __shared__ WarpPairSmem smem[BS / 32];
+    energy_split_body<DIM, BS, true>(c, cnt, st, w, want_tv, smem);
+}
+
 // Capacity guard after the split scan: if the children would not fit, this
 // step runs without splits and reports SPH_ERR_CAPACITY (the reference writes
 // past its buffer, SPH-3D-2/sph_system.cu:1645-1656).
-__global__ void k_split_guard(const sph_config c, Counters *cnt, uint32_t cap)
+__device__ __forceinline__ void split_guard_body(const sph_config &c, Counters *cnt, uint32_t cap)
 {
     uint64_t extra = c.split_ways == 4 ? 3u : 1u;
     uint64_t after = (uint64_t)cnt->n + (uint64_t)cnt->n_split * extra;
@@ -811,6 +884,8 @@ __global__ void k_split_guard(const sph_config c, Counters *cnt, uint32_t cap)
         cnt->split_off = 0u;
     }
 }
+
+__global__ void k_split_guard(const sph_config c, Counters *cnt, uint32_t cap) { split_guard_body(c, cnt, cap); }
 
 // ------------------------------------------------------------ 8. merge
 // One warp per cell over its sorted members (merge_kernel,
@@ -859,10 +934,10 @@ __device__ __forceinline__ void merge_group(const sph_config &c, const WorkPtrs 
         const float4 vv = w.svel_n[t], ee = w.sev_n[t], aa = w.sacc_n[t];
         float ek = w.senergy[t];
         if (sp && ways == 4) ek = ek / 4.0f;
-        P.x += p.x * V[k]; P.y += p.y * V[k]; P.z += p.z * V[k];
-        Vv.x += vv.x * V[k]; Vv.y += vv.y * V[k]; Vv.z += vv.z * V[k];
-        E.x += ee.x * V[k]; E.y += ee.y * V[k]; E.z += ee.z * V[k];
-        A.x += aa.x * V[k]; A.y += aa.y * V[k]; A.z += aa.z * V[k];
+        P.x = __fmaf_rn(p.x, V[k], P.x); P.y = __fmaf_rn(p.y, V[k], P.y); P.z = __fmaf_rn(p.z, V[k], P.z);
+        Vv.x = __fmaf_rn(vv.x, V[k], Vv.x); Vv.y = __fmaf_rn(vv.y, V[k], Vv.y); Vv.z = __fmaf_rn(vv.z, V[k], Vv.z);
+        E.x = __fmaf_rn(ee.x, V[k], E.x); E.y = __fmaf_rn(ee.y, V[k], E.y); E.z = __fmaf_rn(ee.z, V[k], E.z);
+        A.x = __fmaf_rn(aa.x, V[k], A.x); A.y = __fmaf_rn(aa.y, V[k], A.y); A.z = __fmaf_rn(aa.z, V[k], A.z);
         en += ek;
     }
     const uint32_t t1 = g[0];
@@ -879,13 +954,17 @@ __device__ __forceinline__ void merge_group(const sph_config &c, const WorkPtrs 
     }
 }
 
-template <int DIM, int BS = kThreads>
-__global__ void __launch_bounds__(BS) k_merge(sph_config c, const Counters *__restrict__ cnt,
-                                                   CanonPtrs st, WorkPtrs w, uint32_t ncells, uint32_t cap)
+// Shared memory of one warp of the merge pass.
+struct MergeSmem {
+    uint32_t list[kMergeListMax];    // eligible slots in slot order
+    uint32_t lcell[kMergeListMax];   // their cells
+    uint8_t lrank[kMergeListMax];    // their ranks among their cell's eligible members
+};
+
+template <int DIM>
+__device__ __forceinline__ void merge_body(const sph_config &c, const Counters *cnt, const CanonPtrs &st,
+                                           const WorkPtrs &w, uint32_t ncells, uint32_t cap, MergeSmem *ms)
 {
-    __shared__ uint32_t list[BS / 32][kMergeListMax];    // eligible slots in slot order
-    __shared__ uint32_t lcell[BS / 32][kMergeListMax];   // their cells
-    __shared__ uint8_t lrank[BS / 32][kMergeListMax];    // their ranks among their cell's eligible members
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -933,9 +1012,9 @@ __global__ void __launch_bounds__(BS) k_merge(sph_config c, const Counters *__re
             const uint32_t rank = __popc(eb & same & lt) + (cell == carry_cell ? carry_cnt : 0u);
             const uint32_t pos = len + __popc(eb & lt);
             if (el && pos < (uint32_t)kMergeListMax) {
-                list[wib][pos] = t;
-                lcell[wib][pos] = cell;
-                lrank[wib][pos] = (uint8_t)min(rank, 255u);   // a rank inside the list is below its length
+                ms[wib].list[pos] = t;
+                ms[wib].lcell[pos] = cell;
+                ms[wib].lrank[pos] = (uint8_t)min(rank, 255u);   // a rank inside the list is below its length
             }
             len += __popc(eb);
             const int last = __popc(__ballot_sync(full, in)) - 1;
@@ -949,8 +1028,9 @@ __global__ void __launch_bounds__(BS) k_merge(sph_config c, const Counters *__re
             // a group = `ways` consecutive eligible members of one cell, from
             // rank 0 on; its first member is the survivor
             for (uint32_t k = lane; k < len; k += 32)
-                if (lrank[wib][k] % ways == 0 && k + ways - 1 < len && lcell[wib][k + ways - 1] == lcell[wib][k])
-                    merge_group<DIM>(c, w, &list[wib][k], ways, split_on, hs2);
+                if (ms[wib].lrank[k] % ways == 0 && k + ways - 1 < len &&
+                    ms[wib].lcell[k + ways - 1] == ms[wib].lcell[k])
+                    merge_group<DIM>(c, w, &ms[wib].list[k], ways, split_on, hs2);
             __syncwarp();
             continue;
         }
@@ -969,14 +1049,14 @@ __global__ void __launch_bounds__(BS) k_merge(sph_config c, const Counters *__re
                 const int el = t < e ? merge_eligible<DIM>(c, w, t, split_on, ways, cell_score) : 0;
                 const unsigned m = __ballot_sync(full, el);
                 const uint32_t r = count + __popc(m & lt);
-                if (el && r < (uint32_t)kMergeListMax) list[wib][r] = t;
+                if (el && r < (uint32_t)kMergeListMax) ms[wib].list[r] = t;
                 count += __popc(m);
             }
             __syncwarp();
             const uint32_t groups = count / ways;
             if (count <= (uint32_t)kMergeListMax) {
                 for (uint32_t g = lane; g < groups; g += 32)
-                    merge_group<DIM>(c, w, &list[wib][g * ways], ways, split_on, hs2);
+                    merge_group<DIM>(c, w, &ms[wib].list[g * ways], ways, split_on, hs2);
             } else if (lane == 0) {
                 // more eligible members than the list holds: walk the cell
                 // serially with the same group arithmetic
@@ -996,21 +1076,31 @@ __global__ void __launch_bounds__(BS) k_merge(sph_config c, const Counters *__re
     }
 }
 
+template <int DIM, int BS = kThreads>
+__global__ void __launch_bounds__(BS) k_merge(sph_config c, const Counters *__restrict__ cnt,
+                                                   CanonPtrs st, WorkPtrs w, uint32_t ncells, uint32_t cap)
+{
+    __shared__ MergeSmem ms[BS / 32];
+    merge_body<DIM>(c, cnt, st, w, ncells, cap, ms);
+}
+
 // ------------------------------------------------------------ 10. write-out
 // Stable partition by status (rearrange, SPH-3D-2/sph_system.cu:1818-1840):
 // [surviving particles in index order][children in split order][removed].
 // Children follow adaptive_particle_kernel (:1576-1615; 3D-4 :1583-1656;
 // 2D :1133-1160).  Writes the other canonical buffer.
-template <int DIM, int BS = kThreads>
-__global__ void __launch_bounds__(BS) k_write(sph_config c, const Counters *__restrict__ cnt,
-                                                   Counters *__restrict__ cnt_next, CanonPtrs out, WorkPtrs w)
+// ranks = false: the step ran no split and removal scans (split and merge
+// both off), so there are no children and nothing is removed.
+template <int DIM>
+__device__ __forceinline__ void write_body(const sph_config &c, const Counters *cnt, Counters *cnt_next,
+                                           const CanonPtrs &out, const WorkPtrs &w, bool ranks = true)
 {
     const uint32_t n = cnt->n;
-    const uint32_t split_on = cnt->split_off ? 0u : 1u;
+    const uint32_t split_on = ranks && !cnt->split_off ? 1u : 0u;
     const uint32_t ways = c.split_ways == 4 ? 4u : 2u;
     const uint32_t extra = ways - 1u;
     const uint32_t n_split = split_on ? cnt->n_split : 0u;
-    const uint32_t n_removed = cnt->n_removed;
+    const uint32_t n_removed = ranks ? cnt->n_removed : 0u;
     const uint32_t n_after = n + n_split * extra;
     const uint32_t n_live = n_after - n_removed;
     const float hs2 = c.kernel[1] / 2.0f;
@@ -1026,8 +1116,8 @@ __global__ void __launch_bounds__(BS) k_write(sph_config c, const Counters *__re
     for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) {
         const uint32_t s = w.inv[i];
         const uint32_t sp = split_on & w.split_c[i];
-        const uint32_t rm = w.removed_c[i];
-        const uint32_t rr = w.removed_rank[i];
+        const uint32_t rm = ranks ? w.removed_c[i] : 0u;
+        const uint32_t rr = ranks ? w.removed_rank[i] : 0u;
         const uint32_t dst = rm ? n_live + rr : i - rr;
         float4 p = w.spos_n[s], v = w.svel_n[s], e = w.sev_n[s], a = w.sacc_n[s];
         const float4 aux = w.saux[s];
@@ -1075,6 +1165,13 @@ __global__ void __launch_bounds__(BS) k_write(sph_config c, const Counters *__re
             }
         }
     }
+}
+
+template <int DIM, int BS = kThreads>
+__global__ void __launch_bounds__(BS) k_write(sph_config c, const Counters *__restrict__ cnt,
+                                                   Counters *__restrict__ cnt_next, CanonPtrs out, WorkPtrs w)
+{
+    write_body<DIM>(c, cnt, cnt_next, out, w);
 }
 
 // ------------------------------------------------------------ reference-layout records

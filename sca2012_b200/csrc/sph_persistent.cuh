@@ -1,0 +1,170 @@
+// sph_persistent.cuh — the whole step in one cooperative launch.
+//
+// The reference launches every stage of a step separately
+// (SPHSystem::animation, SPH-3D-2/sph_system.cpp:302-404; animate,
+// SPH-2D/sph_system.cpp:190-264), and so does sph_step's ordinary path (about
+// 19 launches, or one replayed CUDA graph of them).  On small scenes the step
+// is then bound by the launches and the drain between them, not by the work.
+// k_step_persistent runs the same stage bodies (sph_kernels.cuh,
+// sph_scan.cuh) in one launch whose blocks are all resident (a cooperative
+// launch), separated by grid-wide barriers:
+//
+//   zero cell counts | hash | scan cells (3 phases) | scatter | reorder |
+//   density | force + integrate | energy + split decision |
+//   [split scan (3 phases) + capacity guard | merge | removal scan (3 phases)] |
+//   write-out
+//
+// (the bracketed stages only when split or merge is on).  Every particle's
+// arithmetic is the ordinary path's, in the same order, so the results are
+// bit for bit those of sph_step's launches.
+//
+// Barrier: each block's thread 0 publishes its writes (fence), increments one
+// arrival counter and polls it (acquire) until all blocks of the launch have
+// arrived at this barrier.  Every poll counts against a limit; a block whose
+// wait runs out sets the launch's abort flag and SPH_ERR_TIMEOUT in the
+// step's error bits, and every block returns at its next barrier, so the
+// kernel always ends.  The input state buffer is never written, but the step
+// that gave up writes no output: the state after a timeout must be restored
+// (sph_set_state).  A step whose input carries the timeout bit does nothing.
+// No stage reads data through the non-coherent path (loads are NC = false),
+// since a stage reads what an earlier stage of the same launch wrote.
+#pragma once
+#include <cstdint>
+#include "../../include/sph/sph.h"
+#include "sph_kernels.cuh"
+#include "sph_scan.cuh"
+
+namespace sph {
+
+// Barrier state of one launch (zeroed before every launch).
+struct GridSync {
+    uint32_t arrived;   // arrivals of all blocks at all barriers so far
+    uint32_t abort;     // 1 once a block gave up waiting
+    uint32_t where;     // the barrier (1-based) at which the first block gave up
+    uint32_t pad;
+};
+
+struct PersistArgs {
+    GridSync *gs;
+    uint32_t spin_limit;     // polls a block makes before giving up at a barrier
+    uint32_t ncells, cap;
+    uint32_t *scan_blocks;   // at least gridDim.x entries
+    uint32_t *scan_grand;    // the cell scan's total
+    int want_tv;             // keep the wavelet-transformed velocity (debug view)
+    int ranks;               // split or merge on: run the split and removal scans
+};
+
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ uint32_t ld_relaxed_gpu(const uint32_t *p)
+{
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Barrier number k (1, 2, ...) of the launch.  Returns false, for the whole
+// block, once any block has given up.
+__device__ __forceinline__ bool grid_barrier(const PersistArgs &a, uint32_t k, Counters *cin, Counters *cout)
+{
+    __shared__ uint32_t s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        GridSync *gs = a.gs;
+        __threadfence();   // the block's writes before its arrival
+        atomicAdd(&gs->arrived, 1u);
+        const uint32_t target = k * gridDim.x;
+        uint32_t ok = 1;
+        for (uint32_t it = 0;; ++it) {
+            if (it >= a.spin_limit || ld_relaxed_gpu(&gs->abort)) {
+                if (atomicExch(&gs->abort, 1u) == 0u) {
+                    gs->where = k;
+                    atomicOr(&cin->error, 1u << SPH_ERR_TIMEOUT);
+                    atomicOr(&cout->error, 1u << SPH_ERR_TIMEOUT);
+                }
+                ok = 0;
+                break;
+            }
+            if (ld_acquire_gpu(&gs->arrived) >= target) break;
+            __nanosleep(64);
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// The three scan phases between barriers: exclusive scan of in[0, len) into
+// out, block totals in a.scan_blocks, grand total to *grand.
+template <typename T>
+__device__ __forceinline__ bool grid_scan(const PersistArgs &a, uint32_t &k, Counters *cin, Counters *cout,
+                                          const T *in, T *out, uint32_t len, T *grand, int total_at_len,
+                                          uint32_t *list)
+{
+    scan_phase1_body<T>(in, len, a.scan_blocks);
+    if (!grid_barrier(a, ++k, cin, cout)) return false;
+    if (blockIdx.x == 0) scan_phase2_body<T>(a.scan_blocks, gridDim.x, grand);
+    if (!grid_barrier(a, ++k, cin, cout)) return false;
+    scan_phase3_body<T>(in, out, len, a.scan_blocks, grand, total_at_len, list);
+    return true;
+}
+
+template <int DIM, int BS>
+__global__ void __launch_bounds__(BS) k_step_persistent(sph_config c, Counters *cin, Counters *cout, CanonPtrs in,
+                                                        CanonPtrs out, WorkPtrs w, PersistArgs a)
+{
+    // one shared buffer for the stages that use shared memory
+    __shared__ union {
+        WarpPairSmem pair[BS / 32];
+        MergeSmem merge[BS / 32];
+    } sm;
+    if (cin->error & (1u << SPH_ERR_TIMEOUT)) {   // a step before gave up: nothing to step from
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&cout->error, cin->error);
+        return;
+    }
+    uint32_t k = 0;
+    for (uint32_t q = grid_stride_start(); q < a.ncells; q += grid_stride()) w.cell_count[q] = 0u;
+    if (!a.ranks && blockIdx.x == 0 && threadIdx.x == 0) {
+        cin->n_split = 0u;
+        cin->n_removed = 0u;
+        cin->split_off = 0u;
+    }
+    if (!grid_barrier(a, ++k, cin, cout)) return;
+    hash_body<DIM>(c, cin, in, w);
+    if (!grid_barrier(a, ++k, cin, cout)) return;
+    if (!grid_scan<uint32_t>(a, k, cin, cout, w.cell_count, w.cell_off, a.ncells, a.scan_grand, 1, nullptr)) return;
+    if (!grid_barrier(a, ++k, cin, cout)) return;
+    scatter_body<false>(cin, w);
+    if (!grid_barrier(a, ++k, cin, cout)) return;
+    reorder_body<false>(cin, in, w);
+    if (!grid_barrier(a, ++k, cin, cout)) return;
+    density_body<DIM, false>(c, cin, w);
+    if (!grid_barrier(a, ++k, cin, cout)) return;
+    force_integrate_body<DIM, BS, false>(c, cin, w, sm.pair);
+    if (!grid_barrier(a, ++k, cin, cout)) return;
+    energy_split_body<DIM, BS, false>(c, cin, in, w, a.want_tv, sm.pair);
+    if (!grid_barrier(a, ++k, cin, cout)) return;
+    if (a.ranks) {
+        const uint32_t n = cin->n;
+        if (!grid_scan<uint32_t>(a, k, cin, cout, w.split_c, w.split_rank, n, &cin->n_split, 0, w.split_list))
+            return;
+        if (blockIdx.x == 0 && threadIdx.x == 0) split_guard_body(c, cin, a.cap);
+        if (!grid_barrier(a, ++k, cin, cout)) return;
+        if (c.use_merge) {
+            merge_body<DIM>(c, cin, in, w, a.ncells, a.cap, sm.merge);
+            if (!grid_barrier(a, ++k, cin, cout)) return;
+        }
+        if (!grid_scan<uint32_t>(a, k, cin, cout, w.removed_c, w.removed_rank, n, &cin->n_removed, 0, nullptr))
+            return;
+        if (!grid_barrier(a, ++k, cin, cout)) return;
+    }
+    write_body<DIM>(c, cin, cout, out, w, a.ranks != 0);
+}
+
+}  // namespace sph

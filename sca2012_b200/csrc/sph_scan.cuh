@@ -69,12 +69,14 @@ __device__ __forceinline__ void chunk_of(uint32_t len, uint32_t &b, uint32_t &e)
     e = min(len, b + chunk);
 }
 
+// The phases as device bodies over the launch's blocks (gridDim.x of them,
+// at most kScanBlocks; blockDim.x at most kScanThreads), shared by the three
+// launches below and by the persistent step kernel, which runs them between
+// grid-wide barriers.
 template <typename T>
-__global__ void __launch_bounds__(kScanThreads) scan_phase1(const T *__restrict__ in, const uint32_t *len_ptr,
-                                                           uint32_t len_const, T *__restrict__ block_tot)
+__device__ __forceinline__ void scan_phase1_body(const T *in, uint32_t len, T *block_tot)
 {
     __shared__ T wt[kScanThreads / 32];
-    const uint32_t len = len_ptr ? *len_ptr : len_const;
     uint32_t b, e;
     chunk_of(len, b, e);
     T acc = zero_of<T>();
@@ -82,6 +84,33 @@ __global__ void __launch_bounds__(kScanThreads) scan_phase1(const T *__restrict_
     T tot;
     block_inclusive_scan(acc, wt, &tot);
     if (threadIdx.x == 0) block_tot[blockIdx.x] = tot;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) scan_phase1(const T *__restrict__ in, const uint32_t *len_ptr,
+                                                           uint32_t len_const, T *__restrict__ block_tot)
+{
+    scan_phase1_body<T>(in, len_ptr ? *len_ptr : len_const, block_tot);
+}
+
+// Exclusive scan of nb block totals by one block of any size (each thread
+// takes a contiguous run); grand total to *grand (if non-null).
+template <typename T>
+__device__ __forceinline__ void scan_phase2_body(T *block_tot, uint32_t nb, T *grand)
+{
+    __shared__ T wt[kScanThreads / 32];
+    const uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
+    const uint32_t b = min(nb, threadIdx.x * per), e = min(nb, b + per);
+    T acc = zero_of<T>();
+    for (uint32_t i = b; i < e; ++i) acc = acc + block_tot[i];
+    T tot;
+    T run = block_inclusive_scan(acc, wt, &tot) - acc;
+    for (uint32_t i = b; i < e; ++i) {
+        const T v = block_tot[i];
+        block_tot[i] = run;
+        run = run + v;
+    }
+    if (threadIdx.x == 0 && grand) *grand = tot;
 }
 
 // One block of kScanBlocks threads: exclusive scan of the block totals;
@@ -101,14 +130,10 @@ __global__ void __launch_bounds__(kScanBlocks) scan_phase2(T *block_tot, T *gran
 // out[len] receives the grand total (used for cell offsets, out[C]).
 // If list != nullptr (T = uint32_t flags only), list[out[i]] = i for in[i]==1.
 template <typename T>
-__global__ void __launch_bounds__(kScanThreads) scan_phase3(const T *__restrict__ in, T *__restrict__ out,
-                                                           const uint32_t *len_ptr, uint32_t len_const,
-                                                           const T *__restrict__ block_off,
-                                                           const T *grand, int out_total_at_len,
-                                                           uint32_t *list)
+__device__ __forceinline__ void scan_phase3_body(const T *in, T *out, uint32_t len, const T *block_off,
+                                                 const T *grand, int out_total_at_len, uint32_t *list)
 {
     __shared__ T wt[kScanThreads / 32];
-    const uint32_t len = len_ptr ? *len_ptr : len_const;
     uint32_t b, e;
     chunk_of(len, b, e);
     T carry = block_off[blockIdx.x];
@@ -127,6 +152,16 @@ __global__ void __launch_bounds__(kScanThreads) scan_phase3(const T *__restrict_
         carry = carry + tot;
     }
     if (out_total_at_len && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[len] = *grand;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) scan_phase3(const T *__restrict__ in, T *__restrict__ out,
+                                                           const uint32_t *len_ptr, uint32_t len_const,
+                                                           const T *__restrict__ block_off,
+                                                           const T *grand, int out_total_at_len,
+                                                           uint32_t *list)
+{
+    scan_phase3_body<T>(in, out, len_ptr ? *len_ptr : len_const, block_off, grand, out_total_at_len, list);
 }
 
 }  // namespace sph

@@ -28,8 +28,10 @@ FLOOR = 1.0
 
 # One record per check_close call: how many particles were compared, how
 # many were held to the field's RMS instead of their own value (|x64| below
-# FLOOR * rms), how many were excluded as ambiguous, and the largest error
-# against each particle's own value among the compared ones.  Written as JSON
+# FLOOR * rms), how many of those pass only because of that floor (error
+# against their own value above RTOL), how many were excluded as ambiguous,
+# and the largest error against its own value among the particles above the
+# RMS.  Written as JSON
 # lines to $SPH_PARITY_REPORT when that is set.
 REPORT = []
 
@@ -68,7 +70,11 @@ def check_close(name, x, ref, mask=None, rtol=RTOL, floor=FLOOR):
     rms = np.sqrt(np.mean(r[ok] ** 2)) if ok.any() else 0.0
     below = ok & (r < floor * rms)
     own = np.where(ok & (r > 0), norm_rows(xs - rs) / np.where(r > 0, r, 1.0), 0.0)
+    # particles that pass only because of the floor: their error against
+    # their own value is above rtol
+    needs_floor = ok & (own > rtol)
     rec = {"name": name, "compared": int(ok.sum()), "held_to_rms": int(below.sum()),
+           "pass_only_by_floor": int(needs_floor.sum()),
            "excluded_ambiguous": int((~sel).sum()), "non_finite_matched": int((sel & nr).sum()),
            "max_err_bound": float(e.max(initial=0.0)),
            "max_err_own_value_above_rms": float(np.where(below, 0.0, own).max(initial=0.0))}

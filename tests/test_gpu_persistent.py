@@ -1,0 +1,106 @@
+"""The persistent step (sph_set_persistent): the whole step as one
+cooperative launch with grid-wide barriers.  It must give the ordinary
+launches' results bit for bit -- plain and adaptive, 2D and 3D, reference
+and SI presets, batched scenes, compensated positions -- and a barrier whose
+wait runs out must end the launch with SPH_ERR_TIMEOUT and leave the handle
+usable (the wait is made to run out by a poll limit of 0, so no GPU ever
+hangs)."""
+import numpy as np
+import pytest
+
+import sca2012_b200 as sph
+from sca2012_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("pos", "vel", "ev", "acc", "dens", "press", "energy", "surface", "level", "interior")
+
+
+def _same(a, b):
+    return a.shape == b.shape and a.tobytes() == b.tobytes()
+
+
+def _cfg(preset, adapt, n):
+    c = sph.preset(preset)
+    c.use_split = c.use_merge = adapt
+    c.max_particle = max(4 * n, 1024)
+    c.grid_every = 0
+    return c
+
+
+CASES = {
+    "dam_2d_plain": (sph.PRESET_DAM_2D, scenes.dam_2d, 0, 200),
+    "dam_2d_adaptive": (sph.PRESET_DAM_2D, scenes.dam_2d, 1, 60),
+    "ref_2d": (sph.PRESET_REF_2D, scenes.ref_init_2d, 1, 30),
+    "ref_3d2": (sph.PRESET_REF_3D2, scenes.ref_box_3d2, 1, 30),
+    "ref_3d4": (sph.PRESET_REF_3D4, scenes.ref_box_3d4, 1, 20),
+    "dam_3d2_block": (sph.PRESET_DAM_3D2, lambda c: scenes.block_3d(c, (24, 24, 12), 0.01, seed=2), 1, 60),
+    "rollout_preset": (sph.PRESET_ROLLOUT_3D, lambda c: scenes.block_3d(c, (16, 16, 16), 0.01, seed=4), 1, 40),
+}
+
+
+def _run(cfg, st0, steps, persistent, scene_boxes=None, debug=False):
+    s = sph.Solver(cfg)
+    if scene_boxes is not None:
+        s.set_scenes(scene_boxes)
+    s.set_state(st0)
+    s.set_persistent(persistent)
+    s.set_debug(debug)
+    s.step(steps)
+    assert s.sync_status() == 0
+    st = s.get_state()
+    dbg = s.get_debug() if debug else None
+    launches = s.last_launch_count()
+    s.close()
+    return st, dbg, launches
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_persistent_equals_ordinary_launches(name, gpu):
+    preset, scene, adapt, steps = CASES[name]
+    pos, vel, lvl = scene(sph.preset(preset))
+    cfg = _cfg(preset, adapt, len(pos))
+    st0 = dict(pos=pos, vel=vel, level=lvl)
+    a, da, la = _run(cfg, st0, steps, False, debug=True)
+    b, db, lb = _run(cfg, st0, steps, True, debug=True)
+    assert lb == steps, "one launch per step"
+    assert la > lb
+    for f in FIELDS:
+        assert _same(a[f], b[f]), f"{name}: {f} differs"
+    for f in ("hash", "index", "nbr_count", "split_flag", "removed", "cell_start", "cell_end", "trans_vel"):
+        assert _same(np.asarray(da[f]), np.asarray(db[f])), f"{name}: debug {f} differs"
+    if adapt:
+        assert (b["level"] == 2).any() or name == "ref_3d4", "no split happened"
+
+
+def test_persistent_batched_scenes(gpu):
+    base = sph.preset(sph.PRESET_DAM_3D2)
+    base.use_split = base.use_merge = 1
+    base.merge_interior_steps = 20
+    cfg, boxes, pos, vel, lvl, scene, _ = scenes.batch_scenes(base, 8, seed=9, n_min=512, n_max=4096)
+    st0 = dict(pos=pos, vel=vel, level=lvl, scene=scene)
+    a, _, _ = _run(cfg, st0, 50, False, boxes)
+    b, _, _ = _run(cfg, st0, 50, True, boxes)
+    for f in FIELDS + ("scene",):
+        assert _same(a[f], b[f]), f
+
+
+def test_persistent_barrier_timeout_is_reported_and_recoverable(gpu):
+    pos, vel, lvl = scenes.dam_2d(sph.preset(sph.PRESET_DAM_2D))
+    cfg = _cfg(sph.PRESET_DAM_2D, 0, len(pos))
+    st0 = dict(pos=pos, vel=vel, level=lvl)
+    ref, _, _ = _run(cfg, st0, 5, False)
+    s = sph.Solver(cfg)
+    s.set_state(st0)
+    s.set_persistent(True, spin_limit=0)   # every barrier wait gives up at its first poll
+    s.step(3)                              # the first step gives up, the next two do nothing
+    assert s.sync_status() == sph.SPH_ERR_TIMEOUT
+    # the handle is usable: restore the state and step normally
+    s.set_state(st0)
+    s.set_persistent(True)
+    s.step(5)
+    assert s.sync_status() == 0
+    got = s.get_state()
+    s.close()
+    for f in FIELDS:
+        assert _same(got[f], ref[f]), f
