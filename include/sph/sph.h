@@ -73,7 +73,9 @@ extern "C" {
 /* merge criteria */
 #define SPH_MERGE_WAVELET    0  /* level 2 and energy*co_energy + surface*co_surface < merge_criteria (SPH-3D-2/sph_system.cu:1694) */
 #define SPH_MERGE_WAVELET_CELL 1 /* 2D: criterion read from the particle whose index equals the cell index (SPH-2D/sph_system.cu:1207) */
-#define SPH_MERGE_INTERIOR   2  /* level 2 and interior (not split-flagged) for merge_interior_steps steps */
+#define SPH_MERGE_INTERIOR   2  /* level 2 and interior (not split-flagged) for merge_interior_steps steps, paired per cell */
+#define SPH_MERGE_SIBLING    3  /* a split group (parent + children, sph_state_view.sibling) merges back when every
+                                   member is level 2 and interior for merge_interior_steps steps */
 
 typedef struct sph_sphere {
     float pos[3];
@@ -121,7 +123,7 @@ typedef struct sph_config {
     uint32_t merge_rule;     /* SPH_MERGE_* */
     uint32_t split_min_neighbors;   /* SPH_SPLIT_DEFICIT */
     float split_density_ratio;      /* SPH_SPLIT_DEFICIT */
-    uint32_t merge_interior_steps;  /* SPH_MERGE_INTERIOR */
+    uint32_t merge_interior_steps;  /* SPH_MERGE_INTERIOR, SPH_MERGE_SIBLING */
     uint32_t split_copies_fields;   /* 1: child copies dens/press/surface (2D) */
 
     /* obstacles and interactive forces (reference integrator / force kernel) */
@@ -159,8 +161,9 @@ typedef struct sph_state_view {
     float *pos, *vel, *ev, *acc;
     float *dens, *press, *energy, *surface;
     uint32_t *level;
-    uint32_t *interior;      /* SPH_MERGE_INTERIOR counter */
+    uint32_t *interior;      /* SPH_MERGE_INTERIOR / SPH_MERGE_SIBLING counter */
     uint32_t *scene;         /* scene index of each particle (batched scenes; 0 otherwise) */
+    uint32_t *sibling;       /* next member of the particle's split group, 0xffffffff for none (NULL: none) */
 } sph_state_view;
 
 /* One scene of a batch: its walled box inside the handle's world and the

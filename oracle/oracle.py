@@ -188,18 +188,20 @@ def energy(cfg, pos_new, vel_new, level, idx, cs, ce):
 
 
 _STATE_F = ("pos", "vel", "ev", "acc", "dens", "press", "energy", "surface")
+_STATE_U = ("level", "interior", "sibling")
+NO_SIBLING = 0xFFFFFFFF
 
 
 def _view(st, n, keep):
     v = abi().StateView()
     v.n = n
-    for k in _STATE_F + ("level", "interior"):
+    for k in _STATE_F + ("level", "interior", "sibling"):
         a = st.get(k)
         if a is None:
             continue
-        a = np.ascontiguousarray(a, np.uint32 if k in ("level", "interior") else np.float32)
+        a = np.ascontiguousarray(a, np.uint32 if k in _STATE_U else np.float32)
         keep.append(a)
-        setattr(v, k, _u(a) if k in ("level", "interior") else _f(a))
+        setattr(v, k, _u(a) if k in _STATE_U else _f(a))
     return v
 
 
@@ -210,6 +212,7 @@ def _alloc_state(cfg, cap):
         st[k] = np.zeros(cap, np.float32)
     st["level"] = np.zeros(cap, np.uint32)
     st["interior"] = np.zeros(cap, np.uint32)
+    st["sibling"] = np.full(cap, NO_SIBLING, np.uint32)
     return st
 
 

@@ -186,7 +186,7 @@ def _si(c, dim, s, ways, dt):
     c.integrator = 2                 # SPH_INTEGRATE_PHYS
     c.kernel_h6_twice = 0
     c.energy_large_kernel = c.energy_skip_close = 1
-    c.split_rule, c.merge_rule = 1, 2   # SPH_SPLIT_DEFICIT, SPH_MERGE_INTERIOR
+    c.split_rule, c.merge_rule = 1, 3   # SPH_SPLIT_DEFICIT, SPH_MERGE_SIBLING
     c.split_min_neighbors = 20 if dim == 3 else 9
     c.split_density_ratio = _f(0.9)
     c.merge_interior_steps = 50

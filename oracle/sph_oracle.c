@@ -21,6 +21,7 @@
 #endif
 
 #define EMPTY_CELL 0xffffffffu
+#define NO_SIBLING 0xffffffffu   /* a particle outside any split group */
 
 static int g_threads = 0;
 
@@ -504,7 +505,7 @@ int64_t oracle_adapt(const sph_config *c, uint32_t n, uint32_t cap, const sph_st
     }
     /* interior counter (SPH_MERGE_INTERIOR) after this step's decision */
     uint32_t *inter = NULL;
-    if (c->merge_rule == SPH_MERGE_INTERIOR) {
+    if (c->merge_rule == SPH_MERGE_INTERIOR || c->merge_rule == SPH_MERGE_SIBLING) {
         inter = (uint32_t *)malloc(sizeof(uint32_t) * (n ? n : 1));
         for (uint32_t i = 0; i < n; ++i) {
             int flagged = (nbr ? nbr[i] : 0u) < c->split_min_neighbors ||
@@ -523,7 +524,55 @@ int64_t oracle_adapt(const sph_config *c, uint32_t n, uint32_t cap, const sph_st
     double *men = (double *)calloc((size_t)(n ? n : 1), sizeof(double));
     uint8_t *leader = (uint8_t *)calloc((size_t)(n ? n : 1), 1);
     for (uint32_t i = 0; i < n; ++i) removed[i] = 0u;
-    if (c->use_merge) {
+    /* one group's merge: V-weighted average into grp[0] (merge_kernel :1742-1777) */
+#define MERGE_GROUP(grp)                                                                            \
+    do {                                                                                            \
+        uint32_t p1 = (grp)[0];                                                                     \
+        double V[4], Vs = 0.0;                                                                      \
+        for (uint32_t k = 0; k < ways; ++k) {                                                       \
+            uint32_t p = (grp)[k];                                                                  \
+            uint32_t l = k == 0 ? 1u : lev[p];                                                      \
+            V[k] = d == 2 ? 1.0 : (double)c->mass[lv(l)] / (double)in->dens[p];                    \
+            Vs += V[k];                                                                             \
+        }                                                                                           \
+        for (int f = 0; f < 4; ++f)                                                                 \
+            for (int a = 0; a < d; ++a) {                                                           \
+                double acc_ = 0.0;                                                                  \
+                for (uint32_t k = 0; k < ways; ++k) {                                               \
+                    uint32_t p = (grp)[k];                                                          \
+                    double val;                                                                     \
+                    if (f == 0) val = a == 0 ? (double)px[p] : (double)in->pos[(size_t)p * d + a];  \
+                    else if (f == 1) val = in->vel[(size_t)p * d + a];                              \
+                    else if (f == 2) val = in->ev[(size_t)p * d + a];                               \
+                    else val = in->acc[(size_t)p * d + a];                                          \
+                    acc_ += val * V[k];                                                             \
+                }                                                                                   \
+                mx[((size_t)p1 * 4 + f) * d + a] = acc_ / Vs;                                       \
+            }                                                                                       \
+        double es = 0.0;                                                                            \
+        for (uint32_t k = 0; k < ways; ++k) es += en[(grp)[k]];                                     \
+        men[p1] = es / (double)ways;                                                                \
+        leader[p1] = 1;                                                                             \
+        for (uint32_t k = 1; k < ways; ++k) removed[(grp)[k]] = 1u;                                 \
+    } while (0)
+    if (c->use_merge && c->merge_rule == SPH_MERGE_SIBLING) {
+        /* a split group (ring through `sibling`) merges back into its member
+         * of smallest index when every one of its `ways` members is level 2
+         * and interior for merge_interior_steps steps; averaged in ring order */
+        for (uint32_t i = 0; i < n; ++i) {
+            if (!(lev[i] != 1u && inter[i] >= c->merge_interior_steps) || !in->sibling) continue;
+            uint32_t grp[4] = {i, 0, 0, 0}, j = in->sibling[i];
+            int ok = 1;
+            for (uint32_t k = 1; k < ways && ok; ++k) {
+                ok = j < n && j > i && lev[j] != 1u && inter[j] >= c->merge_interior_steps;
+                if (ok) {
+                    grp[k] = j;
+                    j = in->sibling[j];
+                }
+            }
+            if (ok && j == i) MERGE_GROUP(grp);
+        }
+    } else if (c->use_merge) {
 #pragma omp parallel for schedule(dynamic, 64) OMP_THREADS
         for (long qq = 0; qq < (long)C; ++qq) {
             const uint32_t q = (uint32_t)qq;
@@ -558,44 +607,22 @@ int64_t oracle_adapt(const sph_config *c, uint32_t n, uint32_t cap, const sph_st
                 if (el) members[cnt++] = p;
             }
             uint32_t groups = cnt / ways;
-            for (uint32_t g = 0; g < groups; ++g) {
-                const uint32_t *grp = members + g * ways;
-                uint32_t p1 = grp[0];
-                double V[4], Vs = 0.0;
-                for (uint32_t k = 0; k < ways; ++k) {
-                    uint32_t p = grp[k];
-                    uint32_t l = k == 0 ? 1u : lev[p];
-                    V[k] = d == 2 ? 1.0 : (double)c->mass[lv(l)] / (double)in->dens[p];
-                    Vs += V[k];
-                }
-                for (int f = 0; f < 4; ++f)
-                    for (int a = 0; a < d; ++a) {
-                        double acc_ = 0.0;
-                        for (uint32_t k = 0; k < ways; ++k) {
-                            uint32_t p = grp[k];
-                            double val;
-                            if (f == 0) val = a == 0 ? (double)px[p] : (double)in->pos[(size_t)p * d + a];
-                            else if (f == 1) val = in->vel[(size_t)p * d + a];
-                            else if (f == 2) val = in->ev[(size_t)p * d + a];
-                            else val = in->acc[(size_t)p * d + a];
-                            acc_ += val * V[k];
-                        }
-                        mx[((size_t)p1 * 4 + f) * d + a] = acc_ / Vs;
-                    }
-                double es = 0.0;
-                for (uint32_t k = 0; k < ways; ++k) es += en[grp[k]];
-                men[p1] = es / (double)ways;
-                leader[p1] = 1;
-                for (uint32_t k = 1; k < ways; ++k) removed[grp[k]] = 1u;
-            }
+            for (uint32_t g = 0; g < groups; ++g) MERGE_GROUP(members + g * ways);
             if (members != mem) free(members);
         }
     }
 
+#undef MERGE_GROUP
     /* ---- compaction: stable partition by status (rearrange :1818-1840) ----
-     * [surviving old particles][children in split order][removed old ones] */
+     * [surviving old particles][children in split order][removed old ones];
+     * split-group links follow their members (removed_before = new index
+     * offset of a survivor) */
     uint32_t n_removed = 0;
-    for (uint32_t i = 0; i < n; ++i) n_removed += removed[i];
+    uint32_t *removed_before = (uint32_t *)malloc(sizeof(uint32_t) * (n ? n : 1));
+    for (uint32_t i = 0; i < n; ++i) {
+        removed_before[i] = n_removed;
+        n_removed += removed[i];
+    }
     uint32_t n_live = (uint32_t)n_after - n_removed;
     uint32_t surv = 0, gone = 0;
     for (uint32_t i = 0; i < n; ++i) {
@@ -614,6 +641,13 @@ int64_t oracle_adapt(const sph_config *c, uint32_t n, uint32_t cap, const sph_st
         out->surface[dst] = in->surface[i];
         out->level[dst] = lev[i];
         if (out->interior) out->interior[dst] = inter ? inter[i] : 0u;
+        if (out->sibling) {
+            uint32_t sib = NO_SIBLING;
+            if (!removed[i] && !leader[i] && in->sibling && in->sibling[i] < n)
+                sib = in->sibling[i] - removed_before[in->sibling[i]];
+            if (split_flag[i]) sib = n - n_removed + rank[i] * extra;   /* the first child */
+            out->sibling[dst] = sib;
+        }
         if (leader[i]) {
             for (int a = 0; a < d; ++a) {
                 out->pos[(size_t)dst * d + a] = (float)mx[((size_t)i * 4 + 0) * d + a];
@@ -647,10 +681,11 @@ int64_t oracle_adapt(const sph_config *c, uint32_t n, uint32_t cap, const sph_st
                 out->surface[cdst] = in->surface[i];
                 out->level[cdst] = 2u;
                 if (out->interior) out->interior[cdst] = 0u;
+                if (out->sibling) out->sibling[cdst] = k + 1 < extra ? cdst + 1 : dst;
             }
         }
     }
-    free(rank); free(px); free(en); free(lev); free(inter);
+    free(rank); free(px); free(en); free(lev); free(inter); free(removed_before);
     free(mx); free(men); free(leader);
     return (int64_t)n_live;
 }
@@ -686,7 +721,7 @@ int64_t oracle_step(const sph_config *c, uint32_t n, uint32_t cap, const sph_sta
     m.pos = mid; m.vel = mid + (size_t)cap * d; m.ev = mid + (size_t)cap * 2 * d;
     m.acc = mid + (size_t)cap * 3 * d; m.dens = mid + (size_t)cap * 4 * d;
     m.press = m.dens + cap; m.energy = m.press + cap; m.surface = m.energy + cap;
-    m.level = in->level; m.interior = in->interior;
+    m.level = in->level; m.interior = in->interior; m.sibling = in->sibling;
     float *lvl_f = m.surface + cap;   /* unused slot kept for layout */
     (void)lvl_f;
     for (size_t i = 0; i < (size_t)n * d; ++i) {

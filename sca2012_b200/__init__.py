@@ -48,8 +48,10 @@ def _u(a):
     return a.ctypes.data_as(_abi.UP) if a is not None else None
 
 
-STATE_FIELDS = ("pos", "vel", "ev", "acc", "dens", "press", "energy", "surface", "level", "interior", "scene")
-_U32_FIELDS = ("level", "interior", "scene")
+STATE_FIELDS = ("pos", "vel", "ev", "acc", "dens", "press", "energy", "surface", "level", "interior", "scene",
+                "sibling")
+_U32_FIELDS = ("level", "interior", "scene", "sibling")
+NO_SIBLING = 0xFFFFFFFF   # sibling of a particle outside any split group
 
 
 def particle_dtype(dim):
@@ -142,7 +144,8 @@ class Solver:
         self._check(self._lib.sph_add_particles(self._h, n, _f(pos), _f(vel), _u(level)), "sph_add_particles")
 
     def set_state(self, st):
-        """st: dict with pos/vel/ev/acc (n x dim) and optional scalars, level (n)."""
+        """st: dict with pos/vel/ev/acc (n x dim) and optional scalars, level (n);
+        `sibling` (the split-group ring) defaults to none."""
         pos = np.ascontiguousarray(st["pos"], np.float32)
         n = pos.shape[0]
         keep = {}
@@ -171,6 +174,7 @@ class Solver:
         out["level"] = np.zeros(n, np.uint32)
         out["interior"] = np.zeros(n, np.uint32)
         out["scene"] = np.zeros(n, np.uint32)
+        out["sibling"] = np.full(n, NO_SIBLING, np.uint32)
         v = StateView()
         v.n = n
         for k in STATE_FIELDS:

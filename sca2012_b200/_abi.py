@@ -32,6 +32,7 @@ SPLIT_DEFICIT = 1
 MERGE_WAVELET = 0
 MERGE_WAVELET_CELL = 1
 MERGE_INTERIOR = 2
+MERGE_SIBLING = 3
 
 F2 = C.c_float * 2
 F3 = C.c_float * 3
@@ -82,7 +83,7 @@ UP = C.POINTER(C.c_uint32)
 class StateView(C.Structure):
     _fields_ = [("n", C.c_uint32), ("pos", FP), ("vel", FP), ("ev", FP), ("acc", FP),
                 ("dens", FP), ("press", FP), ("energy", FP), ("surface", FP),
-                ("level", UP), ("interior", UP), ("scene", UP)]
+                ("level", UP), ("interior", UP), ("scene", UP), ("sibling", UP)]
 
 
 class Scene(C.Structure):

@@ -245,8 +245,13 @@ template <int DIM> int run_step(sph_handle *h)
     SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_REORDER],
                   k_reorder<B><<<grid_st(h, nub, SPH_TUNE_REORDER), B, 0, s>>>(cin, in, w));
     stage(h, "reorder");
-    SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_DENSITY],
-                  k_density<DIM, B><<<grid_st(h, nub, SPH_TUNE_DENSITY), B, 0, s>>>(c, cin, w));
+    if (c.density_skip_r2 == 0.0f) {
+        SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_DENSITY],
+                      k_density<DIM, B, false><<<grid_st(h, nub, SPH_TUNE_DENSITY), B, 0, s>>>(c, cin, w));
+    } else {
+        SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_DENSITY],
+                      k_density<DIM, B, true><<<grid_st(h, nub, SPH_TUNE_DENSITY), B, 0, s>>>(c, cin, w));
+    }
     stage(h, "density");
     SPH_BS_SWITCH2(h->tune_bs[SPH_TUNE_FORCE], h->tune_minb[SPH_TUNE_FORCE],
                    k_force_integrate<DIM, B, M><<<grid_st(h, nub, SPH_TUNE_FORCE), B, 0, s>>>(c, cin, w));
@@ -280,7 +285,7 @@ template <int DIM> int run_step(sph_handle *h)
     scan_u32(h, w.removed_c, w.removed_rank, &cin->n, 0, &cin->n_removed, 0, nullptr);
     stage(h, "scan_removed");
     SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_WRITE],
-                  k_write<DIM, B><<<grid_st(h, nub, SPH_TUNE_WRITE), B, 0, s>>>(c, cin, cout, out, w));
+                  k_write<DIM, B><<<grid_st(h, nub, SPH_TUNE_WRITE), B, 0, s>>>(c, cin, cout, in, out, w));
     h->last_launches += 1;
     stage(h, "write");
     h->cur = p ^ 1;
@@ -419,6 +424,8 @@ int sph_create(const sph_config *cfg, sph_handle **out)
         rc |= dalloc(h, &q.dens, cap); rc |= dalloc(h, &q.press, cap);
         rc |= dalloc(h, &q.energy, cap); rc |= dalloc(h, &q.surface, cap);
         rc |= dalloc(h, &q.interior, cap); rc |= dalloc(h, &q.scene, cap); rc |= dalloc(h, &q.pos_lo, cap);
+        rc |= dalloc(h, &q.sibling, cap);
+        if (!rc) cudaMemset(q.sibling, 0xff, sizeof(uint32_t) * cap);   // no split groups
     }
     WorkPtrs &w = h->w;
     rc |= dalloc(h, &h->cnt, 2);
@@ -557,6 +564,7 @@ int sph_add_particles(sph_handle *h, uint32_t n, const float *pos, const float *
     cudaMemcpyAsync(b.surface + n0, zf.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(b.interior + n0, zu.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(b.scene + n0, zu.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(b.sibling + n0, 0xff, sizeof(uint32_t) * n, s);
     cudaMemsetAsync(b.pos_lo + n0, 0, sizeof(float4) * n, s);
     cudaStreamSynchronize(s);
     write_n(h, n0 + n);
@@ -596,6 +604,8 @@ int sph_set_state(sph_handle *h, const sph_state_view *st)
     cudaMemcpyAsync(b.interior, st->interior ? st->interior : zu.data(), sizeof(uint32_t) * n,
                     cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(b.scene, st->scene ? st->scene : zu.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s);
+    if (st->sibling) cudaMemcpyAsync(b.sibling, st->sibling, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s);
+    else cudaMemsetAsync(b.sibling, 0xff, sizeof(uint32_t) * (n ? n : 1), s);
     cudaMemsetAsync(b.pos_lo, 0, sizeof(float4) * (n ? n : 1), s);
     cudaStreamSynchronize(s);
     write_n(h, n);
@@ -851,6 +861,7 @@ int sph_get_state(sph_handle *h, sph_state_view *st)
     if (st->surface) cudaMemcpy(st->surface, b.surface, sizeof(float) * n, cudaMemcpyDeviceToHost);
     if (st->interior) cudaMemcpy(st->interior, b.interior, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
     if (st->scene) cudaMemcpy(st->scene, b.scene, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
+    if (st->sibling) cudaMemcpy(st->sibling, b.sibling, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost);
     return cuda_check(h, "sph_get_state");
 }
 
@@ -1189,7 +1200,7 @@ int sph_autotune(sph_handle *h, uint32_t reps, sph_tuning *out)
     int bad = talloc(&save.pos, n) | talloc(&save.vel, n) | talloc(&save.ev, n) | talloc(&save.acc, n) |
               talloc(&save.dens, n) | talloc(&save.press, n) | talloc(&save.energy, n) |
               talloc(&save.surface, n) | talloc(&save.interior, n) | talloc(&save.scene, n) |
-              talloc(&save.pos_lo, n);
+              talloc(&save.pos_lo, n) | talloc(&save.sibling, n);
     if (bad) {
         cudaGetLastError();
         for (void *p : tmp) cudaFree(p);
@@ -1204,7 +1215,7 @@ int sph_autotune(sph_handle *h, uint32_t reps, sph_tuning *out)
         c1(d.acc, src.acc, 16ull * n); c1(d.dens, src.dens, 4ull * n); c1(d.press, src.press, 4ull * n);
         c1(d.energy, src.energy, 4ull * n); c1(d.surface, src.surface, 4ull * n);
         c1(d.interior, src.interior, 4ull * n); c1(d.scene, src.scene, 4ull * n);
-        c1(d.pos_lo, src.pos_lo, 16ull * n);
+        c1(d.pos_lo, src.pos_lo, 16ull * n); c1(d.sibling, src.sibling, 4ull * n);
     };
     copy(save, h->buf[h->cur]);
     const int cur0 = h->cur;

@@ -238,7 +238,9 @@ void preset_si(sph_config *c, int dim, float s, uint32_t ways, float dt)
     c->energy_large_kernel = 1;
     c->energy_skip_close = 1;
     c->split_rule = SPH_SPLIT_DEFICIT;
-    c->merge_rule = SPH_MERGE_INTERIOR;
+    // a split group merges back when all its members have been interior for
+    // merge_interior_steps steps (the configs' "children merge back")
+    c->merge_rule = SPH_MERGE_SIBLING;
     // A particle on the simple-cubic lattice at spacing s has 26 neighbours
     // with r < 2s (|d|^2 in {1,2,3}); a free-surface particle keeps at most 17.
     // Fewer than 20 flags a deficit (2D: 12 interior, <= 8 at a face -> < 9).

@@ -51,6 +51,7 @@ struct CanonPtrs {
     float4 *pos, *vel, *ev, *acc;
     float *dens, *press, *energy, *surface;
     uint32_t *interior;
+    uint32_t *sibling;                   // next member of the particle's split group (kEmpty: none)
     uint32_t *scene;                     // scene index (batched scenes)
     float4 *pos_lo;                      // low part of the position (compensated positions)
 };
@@ -389,11 +390,10 @@ __device__ __forceinline__ void warp_pairs(const sph_config &c, const uint32_t *
 // ------------------------------------------------------------ 5. density
 // rho_i = m_i poly6_i h_i^6 + sum_{j != i, skip <= r^2 < h_i^2} m_j poly6_i (h_i^2 - r^2)^3
 // p_i = k ((rho_i / rho0)^3 - 1)         (SPH-3D-2/sph_system.cu:338-677)
-#ifndef SPH_DENS_MINB
-#define SPH_DENS_MINB 1
-#endif
-template <int DIM, bool NC>
-__device__ __forceinline__ void density_body(const sph_config &c, Counters *cnt, const WorkPtrs &w)
+// SKIP = false: the config skips no close pairs (density_skip_r2 == 0), so
+// the test !(r^2 < skip) is true for every r^2 and is left out.
+template <int DIM, bool NC, bool SKIP>
+__device__ __forceinline__ void density_walk(const sph_config &c, Counters *cnt, const WorkPtrs &w)
 {
     const uint32_t n = cnt->n;
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt->disp2_max = 0u;   // the force pass takes the max
@@ -422,26 +422,17 @@ __device__ __forceinline__ void density_body(const sph_config &c, Counters *cnt,
         // fits 32 bits under the lists' 12 GB allocation limit)
         uint32_t *const lbase = rec ? w.nlist + (size_t)s * 4u : nullptr;
         const uint32_t row4 = w.nl_stride * 4u;
-#ifdef SPH_DENS_F2
+        // dx, dy as one packed FP32 subtraction (sm_100 f32x2; each half is the
+        // IEEE round-to-nearest x_j - x_i, so r^2 is r2_of's to the bit)
         const float2 npi = make_float2(-pi.x, -pi.y);
-#endif
         auto add = [&](uint32_t t, float4 pj) {   // t != s (the walk skips s)
-#ifdef SPH_DENS_F2
             const float2 dxy = __fadd2_rn(make_float2(pj.x, pj.y), npi);
             float r2 = __fmaf_rn(dxy.x, dxy.x, __fmul_rn(dxy.y, dxy.y));
             if (DIM == 3) {
                 const float dzz = __fsub_rn(pj.z, pi.z);
                 r2 = __fmaf_rn(dzz, dzz, r2);
             }
-#else
-            float dx, dyy, dzz;
-            const float r2 = r2_of<DIM>(pj, pi, dx, dyy, dzz);
-#endif
-#ifdef SPH_DENS_NOSKIP
-            if (r2 < h2) {
-#else
-            if (!(r2 < skip) && r2 < h2) {
-#endif
+            if ((!SKIP || !(r2 < skip)) && r2 < h2) {
                 const float x = h2 - r2;
                 rho = __fmaf_rn(pj.w == 1.0f ? mp0 : mp1, x * x * x, rho);
                 ++nb;
@@ -490,10 +481,19 @@ __device__ __forceinline__ void density_body(const sph_config &c, Counters *cnt,
     }
 }
 
-template <int DIM, int BS = kThreads>
-__global__ void __launch_bounds__(BS, SPH_DENS_MINB) k_density(sph_config c, Counters *__restrict__ cnt, WorkPtrs w)
+template <int DIM, bool NC>
+__device__ __forceinline__ void density_body(const sph_config &c, Counters *cnt, const WorkPtrs &w)
 {
-    density_body<DIM, true>(c, cnt, w);
+    if (c.density_skip_r2 == 0.0f) density_walk<DIM, NC, false>(c, cnt, w);
+    else density_walk<DIM, NC, true>(c, cnt, w);
+}
+
+// The standalone kernel is instantiated per SKIP (the host picks it): one
+// walk per kernel keeps its registers at the walk's own need.
+template <int DIM, int BS = kThreads, bool SKIP = true>
+__global__ void __launch_bounds__(BS) k_density(sph_config c, Counters *__restrict__ cnt, WorkPtrs w)
+{
+    density_walk<DIM, true, SKIP>(c, cnt, w);
 }
 
 // ------------------------------------------------------------ 6. force + integrate
@@ -855,7 +855,7 @@ __device__ __forceinline__ void energy_split_body(const sph_config &c, Counters 
         }
         w.split_c[i] = split;
         w.removed_c[i] = 0u;
-        if (c.merge_rule == SPH_MERGE_INTERIOR) {
+        if (c.merge_rule == SPH_MERGE_INTERIOR || c.merge_rule == SPH_MERGE_SIBLING) {
             const int flagged = nb < c.split_min_neighbors || dens < c.split_density_ratio * c.rest_density;
             w.sinter[s] = (flagged || split) ? 0u : st.interior[i] + 1u;
         }
@@ -909,7 +909,7 @@ __device__ __forceinline__ int merge_eligible(const sph_config &c, const WorkPtr
         return lvl != 1.0f && split_score(c, en, w.ssurf[t]) < c.merge_criteria;
     }
     if (c.merge_rule == SPH_MERGE_WAVELET_CELL) return lvl == 2.0f && cell_score < c.merge_criteria;
-    return lvl != 1.0f && w.sinter[t] >= c.merge_interior_steps;
+    return lvl != 1.0f && w.sinter[t] >= c.merge_interior_steps;   // SPH_MERGE_INTERIOR, SPH_MERGE_SIBLING
 }
 
 // Merges the group g[0..ways) into g[0] (values on the post-split state).
@@ -1076,12 +1076,47 @@ __device__ __forceinline__ void merge_body(const sph_config &c, const Counters *
     }
 }
 
+// SPH_MERGE_SIBLING: a split group (the parent and its children, linked in a
+// ring by `sibling`) merges back into one particle when all its `ways`
+// members are level 2 and have been interior for merge_interior_steps
+// steps.  The member with the smallest particle index survives; the group
+// is averaged in ring order from it, with merge_group's weights.  One thread
+// per particle; only the survivor-to-be writes, so no group is merged twice.
+template <int DIM>
+__device__ __forceinline__ void merge_sibling_body(const sph_config &c, const Counters *cnt, const CanonPtrs &st,
+                                                   const WorkPtrs &w)
+{
+    const uint32_t n = cnt->n;
+    const uint32_t split_on = cnt->split_off ? 0u : 1u;
+    const uint32_t ways = c.split_ways == 4 ? 4u : 2u;
+    const float hs2 = c.kernel[1] / 2.0f;
+    for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) {
+        const uint32_t si = w.inv[i];
+        if (!merge_eligible<DIM>(c, w, si, split_on, ways, 0.f)) continue;
+        uint32_t g[4];
+        g[0] = si;
+        uint32_t j = st.sibling[i];
+        bool ok = true;
+        for (uint32_t k = 1; k < ways && ok; ++k) {
+            // a ring member of smaller index is the survivor-to-be; it merges
+            ok = j < n && j > i;
+            if (ok) {
+                g[k] = w.inv[j];
+                ok = merge_eligible<DIM>(c, w, g[k], split_on, ways, 0.f);
+                j = st.sibling[j];
+            }
+        }
+        if (ok && j == i) merge_group<DIM>(c, w, g, ways, split_on, hs2);
+    }
+}
+
 template <int DIM, int BS = kThreads>
 __global__ void __launch_bounds__(BS) k_merge(sph_config c, const Counters *__restrict__ cnt,
                                                    CanonPtrs st, WorkPtrs w, uint32_t ncells, uint32_t cap)
 {
     __shared__ MergeSmem ms[BS / 32];
-    merge_body<DIM>(c, cnt, st, w, ncells, cap, ms);
+    if (c.merge_rule == SPH_MERGE_SIBLING) merge_sibling_body<DIM>(c, cnt, st, w);
+    else merge_body<DIM>(c, cnt, st, w, ncells, cap, ms);
 }
 
 // ------------------------------------------------------------ 10. write-out
@@ -1091,9 +1126,13 @@ __global__ void __launch_bounds__(BS) k_merge(sph_config c, const Counters *__re
 // 2D :1133-1160).  Writes the other canonical buffer.
 // ranks = false: the step ran no split and removal scans (split and merge
 // both off), so there are no children and nothing is removed.
+// Split groups: a parent and its children form a ring through `sibling`
+// (parent -> child 0 -> ... -> last child -> parent); a surviving member's
+// link follows the compaction; a merged survivor and everything else has none.
 template <int DIM>
 __device__ __forceinline__ void write_body(const sph_config &c, const Counters *cnt, Counters *cnt_next,
-                                           const CanonPtrs &out, const WorkPtrs &w, bool ranks = true)
+                                           const CanonPtrs &in, const CanonPtrs &out, const WorkPtrs &w,
+                                           bool ranks = true)
 {
     const uint32_t n = cnt->n;
     const uint32_t split_on = ranks && !cnt->split_off ? 1u : 0u;
@@ -1123,7 +1162,7 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
         const float4 aux = w.saux[s];
         float en = w.senergy[s];
         const float sf = w.ssurf[s];
-        uint32_t inter = c.merge_rule == SPH_MERGE_INTERIOR ? w.sinter[s] : 0u;
+        uint32_t inter = (c.merge_rule == SPH_MERGE_INTERIOR || c.merge_rule == SPH_MERGE_SIBLING) ? w.sinter[s] : 0u;
         const float4 p_pre = p;
         if (sp) {
             p.x += hs2;
@@ -1133,6 +1172,12 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
         }
         float4 plo = w.pos_comp ? w.spos_lo_n[s] : make_float4(0.f, 0.f, 0.f, 0.f);
         const float4 plo_pre = plo;
+        uint32_t sib = kEmpty;
+        if (!rm && !w.leader[s]) {
+            const uint32_t j = in.sibling[i];
+            if (j < n) sib = j - (ranks ? w.removed_rank[j] : 0u);
+        }
+        if (sp) sib = n - n_removed + w.split_rank[i] * extra;   // the first child
         if (w.leader[s]) {
             plo = make_float4(0.f, 0.f, 0.f, 0.f);   // a merged position is a fresh FP32 mean
             p = w.mpos[s]; v = w.mvel[s]; e = w.mev[s]; a = w.macc[s];
@@ -1143,6 +1188,7 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
         out.pos[dst] = p; out.vel[dst] = v; out.ev[dst] = e; out.acc[dst] = a;
         out.dens[dst] = aux.x; out.press[dst] = aux.y; out.energy[dst] = en; out.surface[dst] = sf;
         out.interior[dst] = inter;
+        out.sibling[dst] = sib;
         const uint32_t sid = w.nscenes ? w.sscene[s] : 0u;   // a merge group never spans scenes
         if (w.nscenes) out.scene[dst] = sid;
         if (w.pos_comp) out.pos_lo[dst] = plo;
@@ -1160,6 +1206,7 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
                 out.pos[cd] = pc; out.vel[cd] = v0; out.ev[cd] = e0; out.acc[cd] = a0;
                 out.dens[cd] = aux.x; out.press[cd] = aux.y; out.energy[cd] = ec; out.surface[cd] = sf;
                 out.interior[cd] = 0u;
+                out.sibling[cd] = k + 1 < extra ? cd + 1 : dst;
                 if (w.nscenes) out.scene[cd] = sid;
                 if (w.pos_comp) out.pos_lo[cd] = plo_pre;
             }
@@ -1169,9 +1216,10 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
 
 template <int DIM, int BS = kThreads>
 __global__ void __launch_bounds__(BS) k_write(sph_config c, const Counters *__restrict__ cnt,
-                                                   Counters *__restrict__ cnt_next, CanonPtrs out, WorkPtrs w)
+                                                   Counters *__restrict__ cnt_next, CanonPtrs in, CanonPtrs out,
+                                                   WorkPtrs w)
 {
-    write_body<DIM>(c, cnt, cnt_next, out, w);
+    write_body<DIM>(c, cnt, cnt_next, in, out, w);
 }
 
 // ------------------------------------------------------------ reference-layout records
@@ -1250,6 +1298,7 @@ __global__ void __launch_bounds__(kThreads) k_from_aos(uint32_t n, CanonPtrs st,
             st.dens[i] = o[8]; st.press[i] = o[9]; st.energy[i] = o[10]; st.surface[i] = o[12];
         }
         st.interior[i] = 0u;
+        st.sibling[i] = kEmpty;   // nor split groups
         st.scene[i] = 0u;    // the record format carries no scene index
         st.pos_lo[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }

@@ -157,14 +157,15 @@ __global__ void __launch_bounds__(BS) k_step_persistent(sph_config c, Counters *
         if (blockIdx.x == 0 && threadIdx.x == 0) split_guard_body(c, cin, a.cap);
         if (!grid_barrier(a, ++k, cin, cout)) return;
         if (c.use_merge) {
-            merge_body<DIM>(c, cin, in, w, a.ncells, a.cap, sm.merge);
+            if (c.merge_rule == SPH_MERGE_SIBLING) merge_sibling_body<DIM>(c, cin, in, w);
+            else merge_body<DIM>(c, cin, in, w, a.ncells, a.cap, sm.merge);
             if (!grid_barrier(a, ++k, cin, cout)) return;
         }
         if (!grid_scan<uint32_t>(a, k, cin, cout, w.removed_c, w.removed_rank, n, &cin->n_removed, 0, nullptr))
             return;
         if (!grid_barrier(a, ++k, cin, cout)) return;
     }
-    write_body<DIM>(c, cin, cout, out, w, a.ranks != 0);
+    write_body<DIM>(c, cin, cout, in, out, w, a.ranks != 0);
 }
 
 }  // namespace sph

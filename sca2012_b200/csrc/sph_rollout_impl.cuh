@@ -65,7 +65,7 @@ int alloc_canon(sph_handle *h, Rollout *r, CanonPtrs &q)
     rc |= ralloc(h, r, &q.vel, n); rc |= ralloc(h, r, &q.ev, n); rc |= ralloc(h, r, &q.acc, n);
     rc |= ralloc(h, r, &q.dens, n); rc |= ralloc(h, r, &q.press, n); rc |= ralloc(h, r, &q.energy, n);
     rc |= ralloc(h, r, &q.surface, n); rc |= ralloc(h, r, &q.interior, n); rc |= ralloc(h, r, &q.scene, n);
-    rc |= ralloc(h, r, &q.pos_lo, n);
+    rc |= ralloc(h, r, &q.pos_lo, n); rc |= ralloc(h, r, &q.sibling, n);
     return rc ? SPH_ERR_CUDA : SPH_OK;
 }
 
@@ -96,7 +96,7 @@ void copy_canon(const CanonPtrs &dst, const CanonPtrs &src, uint32_t n, cudaStre
     d2d(dst.acc, src.acc, n, s); d2d(dst.dens, src.dens, n, s); d2d(dst.press, src.press, n, s);
     d2d(dst.energy, src.energy, n, s); d2d(dst.surface, src.surface, n, s);
     d2d(dst.interior, src.interior, n, s); d2d(dst.scene, src.scene, n, s);
-    d2d(dst.pos_lo, src.pos_lo, n, s);
+    d2d(dst.pos_lo, src.pos_lo, n, s); d2d(dst.sibling, src.sibling, n, s);
 }
 
 // Makes checkpoint k the handle's current state (all counters reset).

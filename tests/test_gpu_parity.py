@@ -174,11 +174,14 @@ def verify_step(name, cfg_on, cfg, s0, s1, dbg, s1_on, dbg_on):
     # (e) split + merge + compaction from the same post-energy state
     pre = {k: s1[k] for k in ("pos", "vel", "ev", "acc", "dens", "press", "energy", "surface", "level")}
     pre["interior"] = s0["interior"]
+    pre["sibling"] = s0["sibling"]
     exp, split, rem = O.adapt(cfg_on, pre, nbr, idx, cs, ce, cap=cfg_on.max_particle)
     check_equal("split flags", dbg_on["split_flag"], split)
     check_equal("merge flags", dbg_on["removed"], rem)
     assert len(s1_on["pos"]) == len(exp["pos"]), "particle count after split/merge"
     check_equal("levels", s1_on["level"], exp["level"])
+    check_equal("interior counters", s1_on["interior"], exp["interior"])
+    check_equal("split-group links", s1_on["sibling"], exp["sibling"])
     for k in ("pos", "vel", "ev", "acc", "energy"):
         check_close(f"{name}/adapted {k}", s1_on[k], exp[k])
     for k in ("dens", "press", "surface"):
