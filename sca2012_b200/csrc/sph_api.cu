@@ -84,8 +84,12 @@ struct sph_handle {
     // persistent step: the whole step as one cooperative launch
     bool persistent = false;
     uint32_t spin_limit = SPH_PERSISTENT_SPIN_DEFAULT;
-    GridSync *gsync = nullptr;
-    int persist_blocks_per_sm[2] = {0, 0};   // resident blocks of k_step_persistent<2|3> (0: not queried)
+    GridSync *gsync = nullptr;               // [2]: persistent launches alternate between them
+    uint32_t persist_launch = 0;             // persistent launches so far (picks the barrier state)
+    bool counts_zero = false;                // the cell counts are zero (left so by a persistent step)
+    int persist_blocks_per_sm[2][2] = {};    // resident blocks of k_step_persistent<2|3, 64|256> (0: not queried)
+    int persist_cluster_ok[2] = {0, 0};      // one-cluster launches: 1 possible, -1 not, 0 not queried
+    bool persist_use_cluster = true;         // off: always the polled barriers
 };
 
 namespace {
@@ -234,6 +238,7 @@ template <int DIM> int run_step(sph_handle *h)
     if (h->profiling) cudaEventRecord(h->ev[0], s);
 
     cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, s);
+    h->counts_zero = false;   // this step leaves its counts behind
     const uint32_t nub = h->n_ub;
     SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_HASH],
                   k_hash<DIM, B><<<grid_st(h, nub, SPH_TUNE_HASH), B, 0, s>>>(c, cin, in, w));
@@ -245,12 +250,11 @@ template <int DIM> int run_step(sph_handle *h)
     SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_REORDER],
                   k_reorder<B><<<grid_st(h, nub, SPH_TUNE_REORDER), B, 0, s>>>(cin, in, w));
     stage(h, "reorder");
+    const uint32_t gd = grid_st(h, nub, SPH_TUNE_DENSITY);
     if (c.density_skip_r2 == 0.0f) {
-        SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_DENSITY],
-                      k_density<DIM, B, false><<<grid_st(h, nub, SPH_TUNE_DENSITY), B, 0, s>>>(c, cin, w));
+        SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_DENSITY], k_density<DIM, B, false><<<gd, B, 0, s>>>(c, cin, w));
     } else {
-        SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_DENSITY],
-                      k_density<DIM, B, true><<<grid_st(h, nub, SPH_TUNE_DENSITY), B, 0, s>>>(c, cin, w));
+        SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_DENSITY], k_density<DIM, B, true><<<gd, B, 0, s>>>(c, cin, w));
     }
     stage(h, "density");
     SPH_BS_SWITCH2(h->tune_bs[SPH_TUNE_FORCE], h->tune_minb[SPH_TUNE_FORCE],
@@ -298,11 +302,68 @@ template <int DIM> int run_step(sph_handle *h)
 
 // The step as one cooperative launch of k_step_persistent (sph_persistent.cuh):
 // same stages, same arithmetic, grid-wide barriers instead of launch
-// boundaries.  The grid holds one block of 256 threads per 256 particles of
-// the live-count bound, at most what fits resident on the device.
-constexpr int kPersistThreads = 256;
+// boundaries.  One thread per particle of the live-count bound: up to 4,096
+// particles one cluster of 256-thread blocks (hardware cluster barriers),
+// up to 16K blocks of 64 threads (a small scene's stages spread over more
+// SMs), above that blocks of 256; the grid is capped at what fits resident.
+constexpr uint32_t kPersistSmallN = 16384;
+constexpr uint32_t kPersistMaxBlocks = 1024;
 
-template <int DIM> int run_step_persistent(sph_handle *h)
+// A grid of at most kPersistMaxCluster blocks of 256 threads is launched as
+// one cluster when the device can hold it; -1 in cluster_ok: it cannot.
+constexpr uint32_t kPersistMaxCluster = 16;
+
+template <int DIM> int launch_persistent_cluster(sph_handle *h, int &cluster_ok, uint32_t G)
+{
+    const sph_config &c = h->cfg;
+    const int p = h->cur;
+    auto kern = k_step_persistent<DIM, 256>;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(G);
+    lc.blockDim = dim3(256);
+    lc.dynamicSmemBytes = 0;
+    lc.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = G;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    if (cluster_ok == 0) {
+        int n = 0;
+        cluster_ok = -1;
+        if (cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+                cudaSuccess &&
+            cudaOccupancyMaxActiveClusters(&n, (const void *)kern, &lc) == cudaSuccess && n >= 1)
+            cluster_ok = 1;
+        cudaGetLastError();
+        if (cluster_ok < 0) return SPH_ERR_INVALID;
+    }
+    Counters *cin = h->cnt + p, *cout = h->cnt + (p ^ 1);
+    CanonPtrs in = h->buf[p], out = h->buf[p ^ 1];
+    h->w.pos_comp = c.compensated_positions ? 1u : 0u;
+    WorkPtrs w = h->w;
+    if (c.walk_only) w.nlist = w.ncnt = nullptr;
+    // the polled barriers' state is not used; the one due next is left as it
+    // is (clean), so polled launches that follow keep alternating correctly
+    PersistArgs a = {};
+    a.gs = a.gs_next = h->gsync + (h->persist_launch & 1u);
+    a.spin_limit = h->spin_limit;
+    a.ncells = h->ncells;
+    a.cap = h->cap;
+    a.scan_blocks = h->scan_blocks;
+    a.scan_grand = h->scan_grand;
+    a.want_tv = h->debug ? 1 : 0;
+    a.ranks = (c.use_split || c.use_merge) ? 1 : 0;
+    a.cluster = 1;
+    if (!h->counts_zero) cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, h->stream);
+    if (cudaLaunchKernelEx(&lc, kern, c, cin, cout, in, out, w, a) != cudaSuccess)
+        return cuda_check(h, "persistent step cluster launch");
+    return SPH_OK;
+}
+
+template <int DIM, int BS> int launch_persistent(sph_handle *h, int &per_sm, uint32_t G_want)
 {
     const sph_config &c = h->cfg;
     const int p = h->cur;
@@ -311,19 +372,19 @@ template <int DIM> int run_step_persistent(sph_handle *h)
     h->w.pos_comp = c.compensated_positions ? 1u : 0u;
     WorkPtrs w = h->w;
     if (c.walk_only) w.nlist = w.ncnt = nullptr;
-    auto kern = k_step_persistent<DIM, kPersistThreads>;
-    int &per_sm = h->persist_blocks_per_sm[DIM - 2];
+    auto kern = k_step_persistent<DIM, BS>;
     if (per_sm == 0) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPersistThreads, 0) != cudaSuccess ||
-            per_sm < 1) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BS, 0) != cudaSuccess || per_sm < 1) {
             per_sm = 0;
             return cuda_check(h, "persistent step occupancy");
         }
     }
-    const uint32_t want = std::max<uint32_t>(1u, (h->n_ub + kPersistThreads - 1) / kPersistThreads);
-    const uint32_t G = std::min<uint32_t>({want, (uint32_t)(per_sm * h->num_sms), (uint32_t)kScanBlocks});
+    const uint32_t G = std::min<uint32_t>({G_want, (uint32_t)(per_sm * h->num_sms), kPersistMaxBlocks,
+                                           (uint32_t)kScanBlocks});
     PersistArgs a;
-    a.gs = h->gsync;
+    const uint32_t q = h->persist_launch & 1u;
+    a.gs = h->gsync + q;
+    a.gs_next = h->gsync + (q ^ 1u);
     a.spin_limit = h->spin_limit;
     a.ncells = h->ncells;
     a.cap = h->cap;
@@ -331,12 +392,32 @@ template <int DIM> int run_step_persistent(sph_handle *h)
     a.scan_grand = h->scan_grand;
     a.want_tv = h->debug ? 1 : 0;
     a.ranks = (c.use_split || c.use_merge) ? 1 : 0;
+    a.cluster = 0;
     sph_config cc = c;
     void *args[] = {&cc, &cin, &cout, &in, &out, &w, &a};
-    cudaMemsetAsync(h->gsync, 0, sizeof(GridSync), h->stream);
-    if (cudaLaunchCooperativeKernel((void *)kern, dim3(G), dim3(kPersistThreads), args, 0, h->stream) !=
-        cudaSuccess)
+    if (!h->counts_zero) cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, h->stream);
+    if (cudaLaunchCooperativeKernel((void *)kern, dim3(G), dim3(BS), args, 0, h->stream) != cudaSuccess)
         return cuda_check(h, "persistent step launch");
+    return SPH_OK;
+}
+
+template <int DIM> int run_step_persistent(sph_handle *h)
+{
+    const sph_config &c = h->cfg;
+    const int p = h->cur;
+    int rc = SPH_ERR_INVALID;
+    const uint32_t g256 = std::max<uint32_t>(1u, (h->n_ub + 255) / 256);
+    if (g256 <= kPersistMaxCluster && h->persist_cluster_ok[DIM - 2] >= 0 && h->persist_use_cluster)
+        rc = launch_persistent_cluster<DIM>(h, h->persist_cluster_ok[DIM - 2], g256);
+    if (rc != SPH_OK) {
+        if (h->n_ub <= kPersistSmallN)
+            rc = launch_persistent<DIM, 64>(h, h->persist_blocks_per_sm[DIM - 2][0], (h->n_ub + 63) / 64);
+        else
+            rc = launch_persistent<DIM, 256>(h, h->persist_blocks_per_sm[DIM - 2][1], (h->n_ub + 255) / 256);
+        if (rc) return rc;
+        h->persist_launch++;   // the polled barriers alternate between their two states
+    }
+    h->counts_zero = true;   // the write-out stage cleared them
     h->last_launches += 1;
     h->cur = p ^ 1;
     h->step_index++;
@@ -388,6 +469,11 @@ void write_n(sph_handle *h, uint32_t n)
     c0.n = n;
     c0.error &= ~(1u << SPH_ERR_TIMEOUT);   // a new state: steps may run again after a timeout
     cudaMemcpyAsync(&h->cnt[h->cur], &c0, sizeof(Counters), cudaMemcpyHostToDevice, h->stream);
+    // a new state: the persistent step's barrier states start clean (a
+    // timeout leaves its abort flag set) and the cell counts are cleared
+    // before its next launch
+    cudaMemsetAsync(h->gsync, 0, sizeof(GridSync) * 2, h->stream);
+    h->counts_zero = false;
     cudaStreamSynchronize(h->stream);
 }
 
@@ -464,7 +550,7 @@ int sph_create(const sph_config *cfg, sph_handle **out)
     rc |= dalloc(h, &w.macc, cap); rc |= dalloc(h, &w.menergy, cap);
     rc |= dalloc(h, &h->scan_blocks, (size_t)kScanBlocks * 2);
     rc |= dalloc(h, &h->scan_grand, 4);
-    rc |= dalloc(h, &h->gsync, 1);
+    rc |= dalloc(h, &h->gsync, 2);
     if (!rc) rc = mc_alloc(h->mc, *cfg, h->allocs);
     if (rc) {
         fprintf(stderr, "sph_create: %s\n", h->err.c_str());
@@ -699,6 +785,9 @@ int sph_set_persistent(sph_handle *h, int on, uint32_t spin_limit)
     if (!h) return SPH_ERR_INVALID;
     h->persistent = on != 0;
     h->spin_limit = spin_limit;
+    // a wait limit other than the default asks for the polled barriers,
+    // which are the ones a limit applies to
+    h->persist_use_cluster = spin_limit == SPH_PERSISTENT_SPIN_DEFAULT;
     return SPH_OK;
 }
 
@@ -959,11 +1048,7 @@ int sph_write_particles(sph_handle *h, const void *host_src, uint32_t n)
     const uint32_t G = grid_for(h, n);
     if (h->cfg.dim == 3) k_from_aos<3><<<G, kThreads, 0, h->stream>>>(n, h->buf[h->cur], h->aos);
     else k_from_aos<2><<<G, kThreads, 0, h->stream>>>(n, h->buf[h->cur], h->aos);
-    // the count goes through a tiny kernel-free copy on the same stream
-    static thread_local uint32_t n_host;
-    n_host = n;
-    cudaMemcpyAsync(&h->cnt[h->cur].n, &n_host, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream);
-    cudaStreamSynchronize(h->stream);
+    write_n(h, n);
     h->n_ub = n;
     h->have_step = false;
     h->state_gen++;

@@ -9,18 +9,26 @@
 // sph_scan.cuh) in one launch whose blocks are all resident (a cooperative
 // launch), separated by grid-wide barriers:
 //
-//   zero cell counts | hash | scan cells (3 phases) | scatter | reorder |
-//   density | force + integrate | energy + split decision |
-//   [split scan (3 phases) + capacity guard | merge | removal scan (3 phases)] |
-//   write-out
+//   hash | scan cells (2 phases) | scatter | reorder | density |
+//   force + integrate | energy + split decision |
+//   [split scan (2 phases) + capacity guard | merge | removal scan (2 phases)] |
+//   write-out (which also zeroes the cell counts for the next step)
 //
-// (the bracketed stages only when split or merge is on).  Every particle's
+// (the bracketed stages only when split or merge is on): 8 barriers per step
+// without adaptivity, 13 with.  Each scan's second phase has every block sum
+// the block totals itself (scan_phase23_body) instead of one block scanning
+// them between two barriers.  Every particle's
 // arithmetic is the ordinary path's, in the same order, so the results are
 // bit for bit those of sph_step's launches.
 //
-// Barrier: each block's thread 0 publishes its writes (fence), increments one
-// arrival counter and polls it (acquire) until all blocks of the launch have
-// arrived at this barrier.  Every poll counts against a limit; a block whose
+// A grid of at most 16 blocks runs as one thread-block cluster and meets at
+// the hardware cluster barrier instead, which needs no polling.
+// Barrier: each block's thread 0 adds its arrival to one counter with a
+// release add (publishing the block's writes) and polls the counter with
+// acquire loads until all blocks have arrived at this barrier.  Launches
+// alternate between two counters; each launch clears the other one for the
+// next launch, so no memset runs between steps (the host clears both after
+// a timeout).  Every poll counts against a limit; a block whose
 // wait runs out sets the launch's abort flag and SPH_ERR_TIMEOUT in the
 // step's error bits, and every block returns at its next barrier, so the
 // kernel always ends.  The input state buffer is never written, but the step
@@ -36,22 +44,24 @@
 
 namespace sph {
 
-// Barrier state of one launch (zeroed before every launch).
+// Barrier state of one launch (zero when the launch starts).
 struct GridSync {
-    uint32_t arrived;   // arrivals of all blocks at all barriers so far
+    uint32_t arrived;   // arrivals of all blocks at all barriers of the launch
     uint32_t abort;     // 1 once a block gave up waiting
     uint32_t where;     // the barrier (1-based) at which the first block gave up
     uint32_t pad;
 };
 
 struct PersistArgs {
-    GridSync *gs;
+    GridSync *gs;            // this launch's barrier state
+    GridSync *gs_next;       // the next launch's, cleared by this one
     uint32_t spin_limit;     // polls a block makes before giving up at a barrier
     uint32_t ncells, cap;
     uint32_t *scan_blocks;   // at least gridDim.x entries
     uint32_t *scan_grand;    // the cell scan's total
     int want_tv;             // keep the wavelet-transformed velocity (debug view)
     int ranks;               // split or merge on: run the split and removal scans
+    int cluster;             // the grid is one thread-block cluster: hardware cluster barriers
 };
 
 __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p)
@@ -72,12 +82,20 @@ __device__ __forceinline__ uint32_t ld_relaxed_gpu(const uint32_t *p)
 // block, once any block has given up.
 __device__ __forceinline__ bool grid_barrier(const PersistArgs &a, uint32_t k, Counters *cin, Counters *cout)
 {
+    if (a.cluster) {
+        // the whole grid is one cluster, co-scheduled by the hardware: its
+        // barrier (release on arrive, acquire on wait, at cluster scope)
+        // orders every thread's global writes before every later read, and
+        // every thread of every block reaches it, so it needs no limit
+        asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
+                         : "memory");
+        return true;
+    }
     __shared__ uint32_t s_ok;
-    __syncthreads();
+    __syncthreads();   // the block's writes are ordered before thread 0's release
     if (threadIdx.x == 0) {
         GridSync *gs = a.gs;
-        __threadfence();   // the block's writes before its arrival
-        atomicAdd(&gs->arrived, 1u);
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&gs->arrived) : "memory");
         const uint32_t target = k * gridDim.x;
         uint32_t ok = 1;
         for (uint32_t it = 0;; ++it) {
@@ -91,17 +109,15 @@ __device__ __forceinline__ bool grid_barrier(const PersistArgs &a, uint32_t k, C
                 break;
             }
             if (ld_acquire_gpu(&gs->arrived) >= target) break;
-            __nanosleep(64);
         }
-        __threadfence();
         s_ok = ok;
     }
-    __syncthreads();
+    __syncthreads();   // the acquire is ordered before the block's later reads
     return s_ok != 0;
 }
 
-// The three scan phases between barriers: exclusive scan of in[0, len) into
-// out, block totals in a.scan_blocks, grand total to *grand.
+// The scan between barriers: exclusive scan of in[0, len) into out, block
+// totals in a.scan_blocks, grand total to *grand.
 template <typename T>
 __device__ __forceinline__ bool grid_scan(const PersistArgs &a, uint32_t &k, Counters *cin, Counters *cout,
                                           const T *in, T *out, uint32_t len, T *grand, int total_at_len,
@@ -109,14 +125,12 @@ __device__ __forceinline__ bool grid_scan(const PersistArgs &a, uint32_t &k, Cou
 {
     scan_phase1_body<T>(in, len, a.scan_blocks);
     if (!grid_barrier(a, ++k, cin, cout)) return false;
-    if (blockIdx.x == 0) scan_phase2_body<T>(a.scan_blocks, gridDim.x, grand);
-    if (!grid_barrier(a, ++k, cin, cout)) return false;
-    scan_phase3_body<T>(in, out, len, a.scan_blocks, grand, total_at_len, list);
+    scan_phase23_body<T>(in, out, len, a.scan_blocks, grand, total_at_len, list);
     return true;
 }
 
 template <int DIM, int BS>
-__global__ void __launch_bounds__(BS) k_step_persistent(sph_config c, Counters *cin, Counters *cout, CanonPtrs in,
+__global__ void __launch_bounds__(BS, 2) k_step_persistent(sph_config c, Counters *cin, Counters *cout, CanonPtrs in,
                                                         CanonPtrs out, WorkPtrs w, PersistArgs a)
 {
     // one shared buffer for the stages that use shared memory
@@ -128,14 +142,15 @@ __global__ void __launch_bounds__(BS) k_step_persistent(sph_config c, Counters *
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&cout->error, cin->error);
         return;
     }
+    // the cell counts are zero here: the previous persistent step's write-out
+    // cleared them, and the host clears them after any other step
     uint32_t k = 0;
-    for (uint32_t q = grid_stride_start(); q < a.ncells; q += grid_stride()) w.cell_count[q] = 0u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *a.gs_next = GridSync{0u, 0u, 0u, 0u};
     if (!a.ranks && blockIdx.x == 0 && threadIdx.x == 0) {
         cin->n_split = 0u;
         cin->n_removed = 0u;
         cin->split_off = 0u;
     }
-    if (!grid_barrier(a, ++k, cin, cout)) return;
     hash_body<DIM>(c, cin, in, w);
     if (!grid_barrier(a, ++k, cin, cout)) return;
     if (!grid_scan<uint32_t>(a, k, cin, cout, w.cell_count, w.cell_off, a.ncells, a.scan_grand, 1, nullptr)) return;
@@ -166,6 +181,7 @@ __global__ void __launch_bounds__(BS) k_step_persistent(sph_config c, Counters *
         if (!grid_barrier(a, ++k, cin, cout)) return;
     }
     write_body<DIM>(c, cin, cout, in, out, w, a.ranks != 0);
+    for (uint32_t q = grid_stride_start(); q < a.ncells; q += grid_stride()) w.cell_count[q] = 0u;
 }
 
 }  // namespace sph

@@ -216,6 +216,7 @@ template <int DIM> void sort_only(sph_handle *h)
     const uint32_t G = grid_for(h, h->n_ub);
     cudaStream_t s = h->stream;
     cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, s);
+    h->counts_zero = false;
     k_hash<DIM><<<G, kThreads, 0, s>>>(c, cin, in, w);
     scan_u32(h, w.cell_count, w.cell_off, nullptr, h->ncells, h->scan_grand, 1, nullptr);
     k_scatter<<<G, kThreads, 0, s>>>(cin, w);

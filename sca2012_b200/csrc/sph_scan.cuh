@@ -154,6 +154,50 @@ __device__ __forceinline__ void scan_phase3_body(const T *in, T *out, uint32_t l
     if (out_total_at_len && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[len] = *grand;
 }
 
+// Phases 2 and 3 in one: every block sums the nb block totals itself (its
+// exclusive offset and the grand total), then rescans its chunk.  For a grid
+// whose blocks meet at barriers (the persistent step), this saves the barrier
+// after a separate phase 2.  Block 0 writes the grand total to *grand.
+template <typename T>
+__device__ __forceinline__ void scan_phase23_body(const T *in, T *out, uint32_t len, const T *block_tot,
+                                                  T *grand, int out_total_at_len, uint32_t *list)
+{
+    __shared__ T wt[kScanThreads / 32];
+    __shared__ T s_off, s_all;
+    T pre = zero_of<T>(), all = zero_of<T>();
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+        const T v = block_tot[i];
+        all = all + v;
+        if (i < blockIdx.x) pre = pre + v;
+    }
+    T tot;
+    block_inclusive_scan(pre, wt, &tot);
+    if (threadIdx.x == 0) s_off = tot;
+    block_inclusive_scan(all, wt, &tot);
+    if (threadIdx.x == 0) s_all = tot;
+    __syncthreads();
+    const T off = s_off, total = s_all;
+    uint32_t b, e;
+    chunk_of(len, b, e);
+    T carry = off;
+    for (uint32_t base = b; base < e; base += blockDim.x) {
+        uint32_t i = base + threadIdx.x;
+        T v = i < e ? in[i] : zero_of<T>();
+        T t2;
+        T inc = block_inclusive_scan(v, wt, &t2);
+        if (i < e) {
+            T ex = carry + inc - v;
+            out[i] = ex;
+            if constexpr (sizeof(T) == 4) {
+                if (list && v) list[ex] = i;
+            }
+        }
+        carry = carry + t2;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && grand) *grand = total;
+    if (out_total_at_len && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[len] = total;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kScanThreads) scan_phase3(const T *__restrict__ in, T *__restrict__ out,
                                                            const uint32_t *len_ptr, uint32_t len_const,

@@ -4,7 +4,9 @@ launches' results bit for bit -- plain and adaptive, 2D and 3D, reference
 and SI presets, batched scenes, compensated positions -- and a barrier whose
 wait runs out must end the launch with SPH_ERR_TIMEOUT and leave the handle
 usable (the wait is made to run out by a poll limit of 0, so no GPU ever
-hangs)."""
+hangs).  Scenes of up to 4,096 particles run as one thread-block cluster
+with hardware barriers; larger ones, and any wait limit other than the
+default, use the polled barriers."""
 import numpy as np
 import pytest
 
@@ -39,12 +41,12 @@ CASES = {
 }
 
 
-def _run(cfg, st0, steps, persistent, scene_boxes=None, debug=False):
+def _run(cfg, st0, steps, persistent, scene_boxes=None, debug=False, spin_limit=sph._abi.PERSISTENT_SPIN_DEFAULT):
     s = sph.Solver(cfg)
     if scene_boxes is not None:
         s.set_scenes(scene_boxes)
     s.set_state(st0)
-    s.set_persistent(persistent)
+    s.set_persistent(persistent, spin_limit)
     s.set_debug(debug)
     s.step(steps)
     assert s.sync_status() == 0
@@ -71,6 +73,19 @@ def test_persistent_equals_ordinary_launches(name, gpu):
         assert _same(np.asarray(da[f]), np.asarray(db[f])), f"{name}: debug {f} differs"
     if adapt:
         assert (b["level"] == 2).any() or name == "ref_3d4", "no split happened"
+
+
+def test_persistent_polled_and_cluster_barriers_agree(gpu):
+    """4,096 particles fit one 16-block cluster (hardware cluster barriers);
+    a wait limit other than the default selects the polled barriers."""
+    pos, vel, lvl = scenes.dam_2d(sph.preset(sph.PRESET_DAM_2D))
+    cfg = _cfg(sph.PRESET_DAM_2D, 0, len(pos))
+    st0 = dict(pos=pos, vel=vel, level=lvl)
+    a, _, _ = _run(cfg, st0, 100, False)
+    b, _, _ = _run(cfg, st0, 100, True)
+    c, _, _ = _run(cfg, st0, 100, True, spin_limit=1 << 21)
+    for f in FIELDS:
+        assert _same(a[f], b[f]) and _same(a[f], c[f]), f
 
 
 def test_persistent_batched_scenes(gpu):

@@ -24,6 +24,12 @@ FIELDS = ("pos", "vel", "ev", "acc", "dens", "press", "energy", "surface", "leve
 def _case(counts, seed, merge_steps):
     cfg = sph.preset(sph.PRESET_ROLLOUT_3D)
     cfg.merge_interior_steps = merge_steps
+    # level-2 particles of a cell paired in sorted order: this rule merges far
+    # more often than the preset's split-group rule, so the adjoint's merge
+    # path gets the most exercise, and its gradient is large enough that the
+    # 1e-3 relative bound per direction sits above the FP32 trajectory's
+    # rounding (tests/test_gpu_gradcheck_full.py runs the split-group rule)
+    cfg.merge_rule = sph._abi.MERGE_INTERIOR
     pos, _, lvl = scenes.block_3d(cfg, counts=counts, spacing=0.01, seed=seed)
     pos = pos + np.float32(0.1)   # away from the low walls
     rng = np.random.default_rng(seed)
