@@ -210,9 +210,9 @@ def profiled_counters(stage):
     if not os.path.exists(path):
         return None, None, None
     txt = open(path).read()
-    m = re.search(r"traffic_bytes_per_launch_full:\s*([0-9.eE+]+)", txt)
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", txt)
     i = re.search(r"smsp__inst_executed.sum\s+([0-9.]+) M", txt)
-    n = re.search(r"particles_full:\s*([0-9]+)", txt)
+    n = re.search(r"particles:\s*([0-9]+)", txt)
     return ((float(m.group(1)) if m else None), (float(i.group(1)) * 1e6 if i else None),
             (int(n.group(1)) if n else None))
 
@@ -586,7 +586,12 @@ def batched_scenes(args, rank=0, world=1):
     for h in bs:
         h.set_graph(False)
     t_eager = timed(bs, steps)
+    # and as one persistent launch per step (sph_set_persistent)
     for h in bs:
+        h.set_persistent(True)
+    t_persist = timed(bs, steps)
+    for h in bs:
+        h.set_persistent(False)
         h.set_graph(True)
     status = 0
     if world > 1:
@@ -643,7 +648,9 @@ def batched_scenes(args, rank=0, world=1):
             "concurrent_streams_scene_steps_per_s": v_c,
             "batched_vs_sequential": v_b / v_s, "batched_vs_concurrent_streams": v_b / v_c,
             "batched_ms_per_step": t_batched / steps * 1e3,
-            "batched_eager_launches_ms_per_step": t_eager / steps * 1e3, "status": status,
+            "batched_eager_launches_ms_per_step": t_eager / steps * 1e3,
+            "batched_persistent_ms_per_step": t_persist / steps * 1e3,
+            "batched_persistent_scene_steps_per_s": n_sc * steps / t_persist, "status": status,
             "adjoint_last_50": {"forward_ms_per_step": t_fwd / adj_steps * 1e3,
                                 "backward_ms_per_step": t_bwd / adj_steps * 1e3,
                                 "backward_vs_forward": t_bwd / t_fwd,

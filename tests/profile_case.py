@@ -60,7 +60,9 @@ def main():
         cap = [int(x) for x in a.regcap.split(",")] if a.regcap else t["reg_cap"]
         s.set_tuning(block, bpsm, cap)
     s.set_state(dict(pos=pos, vel=vel, level=lvl))
-    s.step(a.steps)
+    for k in range(a.steps):   # the particle count each step starts with (launch k of each kernel)
+        print(f"profile_case: step {k + 1} starts with {s.num_particles()} particles")
+        s.step(1)
     rc = s.sync_status()
     n = s.num_particles()
     s.close()
