@@ -1,7 +1,8 @@
 """Fixed workload runner for profiling the step's kernels under ncu (test tooling).
 
     python tests/profile_case.py [--particles N] [--steps K] [--adaptive 0|1]
-                                 [--block B0,..,B7 --bpsm P0,..,P7]
+                                 [--block B0,..,B7 --bpsm P0,..,P7] [--persistent]
+                                 [--workload dam_3d4|dam_2d]
 
 Runs the four-way dam-break workload for K steps on cuda:0 and exits 0.  By
 default the block is shrunk to about 300,000 particles (inputs still larger
@@ -42,7 +43,21 @@ def main():
     ap.add_argument("--block", default="")
     ap.add_argument("--bpsm", default="")
     ap.add_argument("--regcap", default="")
+    ap.add_argument("--workload", default="dam_3d4", choices=["dam_3d4", "dam_2d"],
+                    help="dam_2d: the 4,096-particle 2D dam (no adaptivity)")
+    ap.add_argument("--persistent", action="store_true", help="run each step as one persistent launch")
     a = ap.parse_args()
+    if a.workload == "dam_2d":
+        cfg = sph.preset(sph.PRESET_DAM_2D)
+        pos, vel, lvl = scenes.dam_2d(cfg, seed=0)
+        s = sph.Solver(cfg)
+        s.set_persistent(a.persistent)
+        s.set_state(dict(pos=pos, vel=vel, level=lvl))
+        s.step(a.steps)
+        rc = s.sync_status()
+        s.close()
+        print(f"profile_case: 2D dam, {a.steps} steps, persistent {a.persistent}, status {rc}")
+        return 0 if rc == 0 else 1
     cfg = sph.preset(sph.PRESET_DAM_3D4)
     pos, vel, lvl = scenes.dam_3d4(cfg)
     if a.particles and a.particles < len(pos):
@@ -53,6 +68,7 @@ def main():
     cfg.use_merge = a.adaptive
     cfg.max_particle = int(len(pos) * 1.5) + 1024
     s = sph.Solver(cfg)
+    s.set_persistent(a.persistent)
     if a.block or a.bpsm or a.regcap:
         t = s.get_tuning()
         block = [int(x) for x in a.block.split(",")] if a.block else t["block"]

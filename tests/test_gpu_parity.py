@@ -116,6 +116,9 @@ DEEP = {
     # 3D two-way dam break at full size (131,072 particles), split and merge
     # on, the 500-step run
     "dam_3d2_run": (sph.PRESET_DAM_3D2, scenes.dam_3d2, 1, (1, 100, 300, 500)),
+    # the 1.1M-particle four-way benchmark workload (block + falling sphere),
+    # the 200-step run, with its surface built every 10 steps as configured
+    "dam_3d4_run": (sph.PRESET_DAM_3D4, scenes.dam_3d4, 1, (1, 100, 200)),
 }
 
 
