@@ -70,7 +70,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     p.add_argument("--batch-scenes", type=int, default=256, help="0 skips the batched-scenes comparison")
-    p.add_argument("--batch-steps", type=int, default=20)
+    p.add_argument("--batch-steps", type=int, default=500, help="batched steps timed (the 500-step run)")
+    p.add_argument("--single-steps", type=int, default=20, help="steps of the one-handle-per-scene baselines")
     p.add_argument("--rollout-steps", type=int, default=200, help="0 skips the differentiable-rollout timing")
     p.add_argument("--other-configs", type=int, default=1, help="0 skips the smaller workloads and CPU detail")
     return p.parse_args()
@@ -531,7 +532,9 @@ def batched_scenes(args, rank=0, world=1):
     """256 independent dam-break scenes (128 2D, 128 3D two-way; sizes
     log-uniform in [1024, 65536], per-scene viscosity and stiffness), split
     and merge on.  Batched: one handle per dimensionality holding all its
-    scenes, each step replayed as a CUDA graph.  Baselines: one handle per
+    scenes, each step replayed as a CUDA graph, over the 500-step run (the
+    same steps are also timed with plain launches and as one persistent
+    launch per step).  Baselines (rates over --single-steps): one handle per
     scene in its own box-sized world with plain (eager) launches, stepped
     (a) one scene at a time, each synchronised before the next, and (b) all
     handles' streams at once.  Scene-steps/s by wall clock around
@@ -633,17 +636,20 @@ def batched_scenes(args, rank=0, world=1):
             sl = slice(first[k], first[k + 1])
             h.set_state(dict(pos=pos[sl] - np.asarray(lo, np.float32), vel=vel[sl], level=lvl[sl]))
             singles.append(h)
+    # the baselines are rates over fewer steps (256 handles one after another
+    # take about 40 ms a step)
     timed(singles, 2)
-    t_seq = timed(singles, steps, per_scene_sync=True)
-    t_conc = timed(singles, steps)
+    s_steps = args.single_steps
+    t_seq = timed(singles, s_steps, per_scene_sync=True)
+    t_conc = timed(singles, s_steps)
     for h in singles:
         status |= h.sync_status()
         h.close()
     n_sc = len(singles)
     v_b = n_sc * steps / t_batched
-    v_s = n_sc * steps / t_seq
-    v_c = n_sc * steps / t_conc
-    return {"scenes": n_sc, "particles_initial": particles, "steps": steps,
+    v_s = n_sc * s_steps / t_seq
+    v_c = n_sc * s_steps / t_conc
+    return {"scenes": n_sc, "particles_initial": particles, "steps": steps, "baseline_steps": s_steps,
             "batched_scene_steps_per_s": v_b, "sequential_scene_steps_per_s": v_s,
             "concurrent_streams_scene_steps_per_s": v_c,
             "batched_vs_sequential": v_b / v_s, "batched_vs_concurrent_streams": v_b / v_c,
