@@ -610,6 +610,8 @@ def batched_scenes(args, rank=0, world=1):
     # density-grid loss over every scene (nodes at cell centres), backward
     t_fwd = t_bwd = 0.0
     adj_steps = 50
+    # the plain batched step at this state (graph replay), the ratio's denominator
+    t_plain_here = timed(bs, adj_steps)
     for h, (cfg, boxes, *_rest) in zip(bs, batches):
         gn = tuple(int(cfg.ncell[a]) for a in range(3))
         org = tuple(0.5 * float(cfg.cell_size) for _ in range(3))
@@ -660,7 +662,8 @@ def batched_scenes(args, rank=0, world=1):
             "adjoint_last_50": {"forward_ms_per_step": t_fwd / adj_steps * 1e3,
                                 "backward_ms_per_step": t_bwd / adj_steps * 1e3,
                                 "backward_vs_forward": t_bwd / t_fwd,
-                                "backward_vs_plain_batched_step": (t_bwd / adj_steps) / (t_batched / steps),
+                                "plain_batched_ms_per_step_here": t_plain_here / adj_steps * 1e3,
+                                "backward_vs_plain_batched_step": t_bwd / t_plain_here,
                                 "loss": "mean squared density grid (nodes at cell centres), per-scene gradients"},
             "timing": "wall clock around synchronised step loops"}
 

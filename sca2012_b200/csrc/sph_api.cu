@@ -87,6 +87,11 @@ struct sph_handle {
     GridSync *gsync = nullptr;               // [2]: persistent launches alternate between them
     uint32_t persist_launch = 0;             // persistent launches so far (picks the barrier state)
     bool counts_zero = false;                // the cell counts are zero (left so by a persistent step)
+    // a persistent step without split and merge leaves the next step's hash
+    // (keys, slots, counts) of the state it wrote; valid while the state, the
+    // config and the step index are the ones it saw
+    bool counts_hashed = false;
+    uint64_t hashed_gen = 0, hashed_step = 0;
     int persist_blocks_per_sm[2][2] = {};    // resident blocks of k_step_persistent<2|3, 64|256> (0: not queried)
     int persist_cluster_ok[2] = {0, 0};      // one-cluster launches: 1 possible, -1 not, 0 not queried
     bool persist_use_cluster = true;         // off: always the polled barriers
@@ -239,6 +244,7 @@ template <int DIM> int run_step(sph_handle *h)
 
     cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, s);
     h->counts_zero = false;   // this step leaves its counts behind
+    h->counts_hashed = false;
     const uint32_t nub = h->n_ub;
     SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_HASH],
                   k_hash<DIM, B><<<grid_st(h, nub, SPH_TUNE_HASH), B, 0, s>>>(c, cin, in, w));
@@ -313,6 +319,11 @@ constexpr uint32_t kPersistMaxBlocks = 1024;
 // one cluster when the device can hold it; -1 in cluster_ok: it cannot.
 constexpr uint32_t kPersistMaxCluster = 16;
 
+static bool hash_ready(const sph_handle *h)
+{
+    return h->counts_hashed && h->hashed_gen == h->state_gen && h->hashed_step == h->step_index;
+}
+
 template <int DIM> int launch_persistent_cluster(sph_handle *h, int &cluster_ok, uint32_t G)
 {
     const sph_config &c = h->cfg;
@@ -357,7 +368,8 @@ template <int DIM> int launch_persistent_cluster(sph_handle *h, int &cluster_ok,
     a.want_tv = h->debug ? 1 : 0;
     a.ranks = (c.use_split || c.use_merge) ? 1 : 0;
     a.cluster = 1;
-    if (!h->counts_zero) cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, h->stream);
+    a.hash_ready = hash_ready(h) ? 1 : 0;
+    if (!a.hash_ready && !h->counts_zero) cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, h->stream);
     if (cudaLaunchKernelEx(&lc, kern, c, cin, cout, in, out, w, a) != cudaSuccess)
         return cuda_check(h, "persistent step cluster launch");
     return SPH_OK;
@@ -393,9 +405,10 @@ template <int DIM, int BS> int launch_persistent(sph_handle *h, int &per_sm, uin
     a.want_tv = h->debug ? 1 : 0;
     a.ranks = (c.use_split || c.use_merge) ? 1 : 0;
     a.cluster = 0;
+    a.hash_ready = hash_ready(h) ? 1 : 0;
     sph_config cc = c;
     void *args[] = {&cc, &cin, &cout, &in, &out, &w, &a};
-    if (!h->counts_zero) cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, h->stream);
+    if (!a.hash_ready && !h->counts_zero) cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, h->stream);
     if (cudaLaunchCooperativeKernel((void *)kern, dim3(G), dim3(BS), args, 0, h->stream) != cudaSuccess)
         return cuda_check(h, "persistent step launch");
     return SPH_OK;
@@ -417,10 +430,16 @@ template <int DIM> int run_step_persistent(sph_handle *h)
         if (rc) return rc;
         h->persist_launch++;   // the polled barriers alternate between their two states
     }
-    h->counts_zero = true;   // the write-out stage cleared them
+    // the scatter stage cleared the counts; without split and merge the
+    // write-out then hashed the new state into them
+    const bool plain = !(c.use_split || c.use_merge);
+    h->counts_zero = !plain;
+    h->counts_hashed = plain;
     h->last_launches += 1;
     h->cur = p ^ 1;
     h->step_index++;
+    h->hashed_gen = h->state_gen;
+    h->hashed_step = h->step_index;
     uint64_t ub = h->n_ub;
     if (c.use_split) ub *= (c.split_ways == 4 ? 4u : 2u);
     h->n_ub = (uint32_t)std::min<uint64_t>(ub, h->cap);
@@ -474,6 +493,7 @@ void write_n(sph_handle *h, uint32_t n)
     // before its next launch
     cudaMemsetAsync(h->gsync, 0, sizeof(GridSync) * 2, h->stream);
     h->counts_zero = false;
+    h->counts_hashed = false;
     cudaStreamSynchronize(h->stream);
 }
 
@@ -764,6 +784,8 @@ int sph_step(sph_handle *h, int nsteps)
             }
             if (cudaGraphLaunch(h->graph[p], h->stream) != cudaSuccess) return cuda_check(h, "cudaGraphLaunch");
             // the bookkeeping run_step does on the host
+            h->counts_zero = false;
+            h->counts_hashed = false;
             h->cur = p ^ 1;
             h->step_index++;
             uint64_t ub = h->n_ub;
@@ -1311,6 +1333,7 @@ int sph_autotune(sph_handle *h, uint32_t reps, sph_tuning *out)
     drop_graphs(h);
     sph_set_profiling(h, 1);
     auto restore = [&]() {
+        h->counts_hashed = false;
         h->cur = cur0;
         copy(h->buf[h->cur], save);
         Counters c0;

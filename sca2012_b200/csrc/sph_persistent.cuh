@@ -9,13 +9,15 @@
 // sph_scan.cuh) in one launch whose blocks are all resident (a cooperative
 // launch), separated by grid-wide barriers:
 //
-//   hash | scan cells (2 phases) | scatter | reorder | density |
-//   force + integrate | energy + split decision |
+//   hash | scan cells (2 phases) | scatter (and clear the counts) | reorder |
+//   density | force + integrate | energy + split decision |
 //   [split scan (2 phases) + capacity guard | merge | removal scan (2 phases)] |
-//   write-out (which also zeroes the cell counts for the next step)
+//   write-out
 //
-// (the bracketed stages only when split or merge is on): 8 barriers per step
-// without adaptivity, 13 with.  Each scan's second phase has every block sum
+// (the bracketed stages only when split or merge is on): 13 barriers per step
+// with adaptivity.  Without it the write-out runs in the energy stage and
+// hashes the next step's state too (write_hash_by_slot_body), so the next
+// launch starts at the scan: 6 barriers per step.  Each scan's second phase has every block sum
 // the block totals itself (scan_phase23_body) instead of one block scanning
 // them between two barriers.  Every particle's
 // arithmetic is the ordinary path's, in the same order, so the results are
@@ -62,7 +64,62 @@ struct PersistArgs {
     int want_tv;             // keep the wavelet-transformed velocity (debug view)
     int ranks;               // split or merge on: run the split and removal scans
     int cluster;             // the grid is one thread-block cluster: hardware cluster barriers
+    int hash_ready;          // the previous launch hashed this step's state already
 };
+
+// Without split and merge (ranks = 0) the write-out needs no global step:
+// particle i = sidx[s] goes to index i, and every value it writes was made for
+// slot s by the same thread (density, force and energy give slot s to the
+// same thread, and so does this loop).  So the thread that finished slot s's
+// energy writes the particle out right away, and hashes its new position for
+// the next step (the counts were cleared after this step's scan).  Values are
+// write_body's for a particle that neither splits nor merges.
+template <int DIM, int BS>
+__device__ __forceinline__ void write_hash_by_slot_body(const sph_config &c, const Counters *cnt, Counters *cnt_next,
+                                                        const CanonPtrs &in, const CanonPtrs &out, const WorkPtrs &w)
+{
+    const uint32_t n = cnt->n;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        cnt_next->n = n;
+        cnt_next->error = cnt->error;
+        cnt_next->n_split = 0;
+        cnt_next->n_removed = 0;
+        cnt_next->split_off = 0;
+    }
+    const bool inter_rule = c.merge_rule == SPH_MERGE_INTERIOR || c.merge_rule == SPH_MERGE_SIBLING;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    for (uint32_t base = blockIdx.x * BS + wib * 32u; base < n; base += gridDim.x * BS) {
+        const uint32_t s = base + lane;
+        const bool valid = s < n;
+        uint32_t k = 0;
+        uint32_t i = 0;
+        if (valid) {
+            i = w.sidx[s];
+            const float4 p = w.spos_n[s];
+            const float4 aux = w.saux[s];
+            out.pos[i] = p; out.vel[i] = w.svel_n[s]; out.ev[i] = w.sev_n[s]; out.acc[i] = w.sacc_n[s];
+            out.dens[i] = aux.x; out.press[i] = aux.y; out.energy[i] = w.senergy[s]; out.surface[i] = w.ssurf[s];
+            out.interior[i] = inter_rule ? w.sinter[s] : 0u;
+            const uint32_t j = in.sibling[i];
+            out.sibling[i] = j < n ? j : kEmpty;
+            if (w.nscenes) out.scene[i] = w.sscene[s];
+            if (w.pos_comp) out.pos_lo[i] = w.spos_lo_n[s];
+            const uint3 q = cell_of<DIM>(c, p);
+            k = key_of(c, q.x, q.y, q.z);
+        }
+        // the next step's hash of particle i (hash_body's slot assignment)
+        const unsigned vm = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+            w.key[i] = k;
+            const unsigned grp = __match_any_sync(vm, k);
+            const int lead = __ffs(grp) - 1;
+            uint32_t first = 0;
+            if (lane == lead) first = atomicAdd(w.cell_count + k, (uint32_t)__popc(grp));
+            first = __shfl_sync(grp, first, lead);
+            w.slot[i] = first + __popc(grp & ((1u << lane) - 1u));
+        }
+    }
+}
 
 __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p)
 {
@@ -151,11 +208,15 @@ __global__ void __launch_bounds__(BS, 2) k_step_persistent(sph_config c, Counter
         cin->n_removed = 0u;
         cin->split_off = 0u;
     }
-    hash_body<DIM>(c, cin, in, w);
-    if (!grid_barrier(a, ++k, cin, cout)) return;
+    if (!a.hash_ready) {
+        hash_body<DIM>(c, cin, in, w);
+        if (!grid_barrier(a, ++k, cin, cout)) return;
+    }
     if (!grid_scan<uint32_t>(a, k, cin, cout, w.cell_count, w.cell_off, a.ncells, a.scan_grand, 1, nullptr)) return;
     if (!grid_barrier(a, ++k, cin, cout)) return;
     scatter_body<false>(cin, w);
+    // no stage reads the counts after the scan: clear them for the next hash
+    for (uint32_t q = grid_stride_start(); q < a.ncells; q += grid_stride()) w.cell_count[q] = 0u;
     if (!grid_barrier(a, ++k, cin, cout)) return;
     reorder_body<false>(cin, in, w);
     if (!grid_barrier(a, ++k, cin, cout)) return;
@@ -164,8 +225,12 @@ __global__ void __launch_bounds__(BS, 2) k_step_persistent(sph_config c, Counter
     force_integrate_body<DIM, BS, false>(c, cin, w, sm.pair);
     if (!grid_barrier(a, ++k, cin, cout)) return;
     energy_split_body<DIM, BS, false>(c, cin, in, w, a.want_tv, sm.pair);
+    if (!a.ranks) {
+        write_hash_by_slot_body<DIM, BS>(c, cin, cout, in, out, w);
+        return;
+    }
     if (!grid_barrier(a, ++k, cin, cout)) return;
-    if (a.ranks) {
+    {
         const uint32_t n = cin->n;
         if (!grid_scan<uint32_t>(a, k, cin, cout, w.split_c, w.split_rank, n, &cin->n_split, 0, w.split_list))
             return;
@@ -180,8 +245,7 @@ __global__ void __launch_bounds__(BS, 2) k_step_persistent(sph_config c, Counter
             return;
         if (!grid_barrier(a, ++k, cin, cout)) return;
     }
-    write_body<DIM>(c, cin, cout, in, out, w, a.ranks != 0);
-    for (uint32_t q = grid_stride_start(); q < a.ncells; q += grid_stride()) w.cell_count[q] = 0u;
+    write_body<DIM>(c, cin, cout, in, out, w, true);
 }
 
 }  // namespace sph

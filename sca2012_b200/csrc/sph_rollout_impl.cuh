@@ -110,6 +110,7 @@ int restore_ckpt(sph_handle *h, Rollout *r, size_t k)
     cudaMemcpyAsync(&h->cnt[h->cur], &c0, sizeof(Counters), cudaMemcpyHostToDevice, h->stream);
     cudaStreamSynchronize(h->stream);
     h->n_ub = n;
+    h->counts_hashed = false;   // the hash a persistent step left is not this state's
     return cuda_check(h, "rollout: restore checkpoint");
 }
 
@@ -217,6 +218,7 @@ template <int DIM> void sort_only(sph_handle *h)
     cudaStream_t s = h->stream;
     cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, s);
     h->counts_zero = false;
+    h->counts_hashed = false;
     k_hash<DIM><<<G, kThreads, 0, s>>>(c, cin, in, w);
     scan_u32(h, w.cell_count, w.cell_off, nullptr, h->ncells, h->scan_grand, 1, nullptr);
     k_scatter<<<G, kThreads, 0, s>>>(cin, w);

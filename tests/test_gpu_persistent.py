@@ -6,7 +6,9 @@ wait runs out must end the launch with SPH_ERR_TIMEOUT and leave the handle
 usable (the wait is made to run out by a poll limit of 0, so no GPU ever
 hangs).  Scenes of up to 4,096 particles run as one thread-block cluster
 with hardware barriers; larger ones, and any wait limit other than the
-default, use the polled barriers."""
+default, use the polled barriers.  Without split and merge a persistent step
+also hashes the state it wrote for the next one; that hash must be dropped
+whenever anything else touches the state, the config or the cell counts."""
 import numpy as np
 import pytest
 
@@ -38,6 +40,8 @@ CASES = {
     "ref_3d4": (sph.PRESET_REF_3D4, scenes.ref_box_3d4, 1, 20),
     "dam_3d2_block": (sph.PRESET_DAM_3D2, lambda c: scenes.block_3d(c, (24, 24, 12), 0.01, seed=2), 1, 60),
     "rollout_preset": (sph.PRESET_ROLLOUT_3D, lambda c: scenes.block_3d(c, (16, 16, 16), 0.01, seed=4), 1, 40),
+    # above 16K particles: the polled barriers with 256-thread blocks, plain
+    "dam_3d2_plain_32k": (sph.PRESET_DAM_3D2, lambda c: scenes.block_3d(c, (40, 40, 20), 0.01, seed=5), 0, 60),
 }
 
 
@@ -119,3 +123,54 @@ def test_persistent_barrier_timeout_is_reported_and_recoverable(gpu):
     s.close()
     for f in FIELDS:
         assert _same(got[f], ref[f]), f
+
+
+def test_persistent_precomputed_hash_follows_state_changes(gpu):
+    """Plain persistent steps interleaved with graph replays, eager steps,
+    a config change, a state reload and a switch of barrier kind give the
+    ordinary launches' bits at every checkpoint."""
+    pos, vel, lvl = scenes.dam_2d(sph.preset(sph.PRESET_DAM_2D))
+    cfg = _cfg(sph.PRESET_DAM_2D, 0, len(pos))
+    st0 = dict(pos=pos, vel=vel, level=lvl)
+    cfg2 = _cfg(sph.PRESET_DAM_2D, 0, len(pos))
+    cfg2.viscosity = cfg.viscosity * 1.5
+
+    def script(s, persistent):
+        out = []
+        s.set_state(st0)
+        s.set_persistent(persistent)
+        s.step(7)
+        out.append(s.get_state())
+        s.set_persistent(False)          # graph replay from a hashed state
+        s.step(3)
+        s.set_persistent(persistent)
+        s.step(4)
+        s.set_graph(False)               # eager launches in between
+        s.set_persistent(False)
+        s.step(2)
+        s.set_graph(True)
+        s.set_persistent(persistent)
+        s.step(5)
+        out.append(s.get_state())
+        s.set_config(cfg2)               # the config changes between two persistent steps
+        s.step(6)
+        out.append(s.get_state())
+        s.set_persistent(persistent, 1 << 21)   # polled barriers from a hash the cluster path left
+        s.step(6)
+        mid = s.get_state()
+        out.append(mid)
+        s.set_state(dict(pos=mid["pos"], vel=mid["vel"] * 0.5, level=mid["level"]))   # reload
+        s.step(5)
+        out.append(s.get_state())
+        assert s.sync_status() == 0
+        return out
+
+    sa = sph.Solver(cfg)
+    a = script(sa, False)
+    sa.close()
+    sb = sph.Solver(cfg)
+    b = script(sb, True)
+    sb.close()
+    for k, (x, y) in enumerate(zip(a, b)):
+        for f in FIELDS:
+            assert _same(x[f], y[f]), f"checkpoint {k}: {f} differs"
