@@ -400,6 +400,42 @@ def run_ours(args, rank, world, local_rank):
         n_cur = n_next
     e2e_t, e2e_ps = reduce_over_ranks(e2e_t, e2e_ps, dist, "cuda")
     e2e_value = e2e_ps / (e2e_t * 1e-3)
+
+    # --- the reference app's frame loop: a step, then the step's records read
+    # back for display (SPH-3D-2/sph_main.cpp:613-733), no upload.  Synchronous
+    # (sph_read_particles) and asynchronous (sph_read_particles_async into
+    # mapped page-locked memory, two buffers, overlapping the next step).
+    frame = {}
+    fbufs = [host, torch.empty(cap_bytes, dtype=torch.uint8, pin_memory=True)]
+    fcnts = [torch.zeros(1, dtype=torch.int32, pin_memory=True) for _ in range(2)]
+    for mode in ("sync", "async"):
+        torch.cuda.synchronize()
+        n_sum, d2h_f = 0, 0
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        n_first = s.num_particles()
+        for k in range(e2e_steps):
+            s.step(1)
+            if mode == "sync":
+                n_here = s.read_particles_into(host.data_ptr(), cap_bytes)
+                n_sum += n_here
+                d2h_f += n_here * rec
+            else:
+                rc = s._lib.sph_read_particles_async(s._h, fbufs[k & 1].data_ptr(), cap_bytes,
+                                                     fcnts[k & 1].data_ptr())
+                assert rc == 0, s._lib.sph_last_error(s._h)
+        if mode == "async":
+            assert s._lib.sph_readback_wait(s._h) == 0
+        b.record(stream)
+        b.synchronize()
+        if mode == "async":   # the count moves by well under 1 % over these steps
+            n_sum = e2e_steps * (n_first + s.num_particles()) // 2
+            d2h_f = n_sum * rec
+        ft, fps = reduce_over_ranks(a.elapsed_time(b), n_sum, dist, "cuda")
+        frame[mode] = {"value": fps / (ft * 1e-3), "unit": UNIT, "ms_per_step": ft / e2e_steps,
+                       "d2h_bytes_per_step": d2h_f // e2e_steps}
+    frame["api"] = ("sph_step + sph_read_particles (sync) / sph_read_particles_async into mapped memory "
+                    "(async); the L2 is not flushed between these steps")
     status |= s.sync_status()
     s.close()
 
@@ -451,7 +487,8 @@ def run_ours(args, rank, world, local_rank):
             "plain_value": plain_value, "adaptive_vs_plain": value / plain_value,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // e2e_steps,
                     "d2h_bytes_per_step": d2h // e2e_steps,
-                    "api": "sph_write_particles + sph_step + sph_read_particles (page-locked host)"},
+                    "api": "sph_write_particles + sph_step + sph_read_particles (page-locked host)",
+                    "frame_loop": frame},
             "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_particle": STAGE_BYTES.get(top),

@@ -324,7 +324,7 @@ static bool hash_ready(const sph_handle *h)
     return h->counts_hashed && h->hashed_gen == h->state_gen && h->hashed_step == h->step_index;
 }
 
-template <int DIM> int launch_persistent_cluster(sph_handle *h, int &cluster_ok, uint32_t G)
+template <int DIM> int launch_persistent_cluster(sph_handle *h, int &cluster_ok, uint32_t G, int nsteps)
 {
     const sph_config &c = h->cfg;
     const int p = h->cur;
@@ -351,8 +351,7 @@ template <int DIM> int launch_persistent_cluster(sph_handle *h, int &cluster_ok,
         cudaGetLastError();
         if (cluster_ok < 0) return SPH_ERR_INVALID;
     }
-    Counters *cin = h->cnt + p, *cout = h->cnt + (p ^ 1);
-    CanonPtrs in = h->buf[p], out = h->buf[p ^ 1];
+    const CanonPair buf = {{h->buf[0], h->buf[1]}};
     h->w.pos_comp = c.compensated_positions ? 1u : 0u;
     WorkPtrs w = h->w;
     if (c.walk_only) w.nlist = w.ncnt = nullptr;
@@ -369,18 +368,20 @@ template <int DIM> int launch_persistent_cluster(sph_handle *h, int &cluster_ok,
     a.ranks = (c.use_split || c.use_merge) ? 1 : 0;
     a.cluster = 1;
     a.hash_ready = hash_ready(h) ? 1 : 0;
+    a.parity = p;
+    a.nsteps = nsteps;
     if (!a.hash_ready && !h->counts_zero) cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, h->stream);
-    if (cudaLaunchKernelEx(&lc, kern, c, cin, cout, in, out, w, a) != cudaSuccess)
+    if (cudaLaunchKernelEx(&lc, kern, c, h->cnt, buf, w, a) != cudaSuccess)
         return cuda_check(h, "persistent step cluster launch");
     return SPH_OK;
 }
 
-template <int DIM, int BS> int launch_persistent(sph_handle *h, int &per_sm, uint32_t G_want)
+template <int DIM, int BS> int launch_persistent(sph_handle *h, int &per_sm, uint32_t G_want, int nsteps)
 {
     const sph_config &c = h->cfg;
     const int p = h->cur;
-    Counters *cin = h->cnt + p, *cout = h->cnt + (p ^ 1);
-    CanonPtrs in = h->buf[p], out = h->buf[p ^ 1];
+    Counters *cnt = h->cnt;
+    CanonPair buf = {{h->buf[0], h->buf[1]}};
     h->w.pos_comp = c.compensated_positions ? 1u : 0u;
     WorkPtrs w = h->w;
     if (c.walk_only) w.nlist = w.ncnt = nullptr;
@@ -406,27 +407,35 @@ template <int DIM, int BS> int launch_persistent(sph_handle *h, int &per_sm, uin
     a.ranks = (c.use_split || c.use_merge) ? 1 : 0;
     a.cluster = 0;
     a.hash_ready = hash_ready(h) ? 1 : 0;
+    a.parity = p;
+    a.nsteps = nsteps;
     sph_config cc = c;
-    void *args[] = {&cc, &cin, &cout, &in, &out, &w, &a};
+    void *args[] = {&cc, &cnt, &buf, &w, &a};
     if (!a.hash_ready && !h->counts_zero) cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, h->stream);
     if (cudaLaunchCooperativeKernel((void *)kern, dim3(G), dim3(BS), args, 0, h->stream) != cudaSuccess)
         return cuda_check(h, "persistent step launch");
     return SPH_OK;
 }
 
-template <int DIM> int run_step_persistent(sph_handle *h)
+// Steps one persistent launch runs at most.  Only steps whose particle count
+// cannot grow (no splits) share a launch: the grid is sized for the count
+// the first step starts from.
+constexpr int kPersistMaxSteps = 256;
+
+template <int DIM> int run_step_persistent(sph_handle *h, int nsteps)
 {
     const sph_config &c = h->cfg;
     const int p = h->cur;
     int rc = SPH_ERR_INVALID;
     const uint32_t g256 = std::max<uint32_t>(1u, (h->n_ub + 255) / 256);
     if (g256 <= kPersistMaxCluster && h->persist_cluster_ok[DIM - 2] >= 0 && h->persist_use_cluster)
-        rc = launch_persistent_cluster<DIM>(h, h->persist_cluster_ok[DIM - 2], g256);
+        rc = launch_persistent_cluster<DIM>(h, h->persist_cluster_ok[DIM - 2], g256, nsteps);
     if (rc != SPH_OK) {
         if (h->n_ub <= kPersistSmallN)
-            rc = launch_persistent<DIM, 64>(h, h->persist_blocks_per_sm[DIM - 2][0], (h->n_ub + 63) / 64);
+            rc = launch_persistent<DIM, 64>(h, h->persist_blocks_per_sm[DIM - 2][0], (h->n_ub + 63) / 64, nsteps);
         else
-            rc = launch_persistent<DIM, 256>(h, h->persist_blocks_per_sm[DIM - 2][1], (h->n_ub + 255) / 256);
+            rc = launch_persistent<DIM, 256>(h, h->persist_blocks_per_sm[DIM - 2][1], (h->n_ub + 255) / 256,
+                                             nsteps);
         if (rc) return rc;
         h->persist_launch++;   // the polled barriers alternate between their two states
     }
@@ -436,12 +445,12 @@ template <int DIM> int run_step_persistent(sph_handle *h)
     h->counts_zero = !plain;
     h->counts_hashed = plain;
     h->last_launches += 1;
-    h->cur = p ^ 1;
-    h->step_index++;
+    h->cur = (p + nsteps) & 1;
+    h->step_index += (uint64_t)nsteps;
     h->hashed_gen = h->state_gen;
     h->hashed_step = h->step_index;
     uint64_t ub = h->n_ub;
-    if (c.use_split) ub *= (c.split_ways == 4 ? 4u : 2u);
+    if (c.use_split) ub *= (c.split_ways == 4 ? 4u : 2u);   // one step per launch then
     h->n_ub = (uint32_t)std::min<uint64_t>(ub, h->cap);
     return cuda_check(h, "sph_step persistent");
 }
@@ -763,6 +772,9 @@ int sph_step(sph_handle *h, int nsteps)
 {
     if (!h || nsteps < 0) return SPH_ERR_INVALID;
     h->last_launches = 0;
+    auto surface_due = [h](uint64_t step) {
+        return h->cfg.dim == 3 && h->cfg.grid_every && h->mc.nodes && step % h->cfg.grid_every == 0;
+    };
     for (int k = 0; k < nsteps; ++k) {
         if (h->n_ub == 0) break;
         h->n_last_sorted = 0;   // resolved lazily by sph_get_debug
@@ -771,12 +783,20 @@ int sph_step(sph_handle *h, int nsteps)
             cudaStreamWaitEvent(h->stream, h->rb_done[h->cur ^ 1], 0);
             h->rb_pending[h->cur ^ 1] = false;
         }
-        const bool surface_due = h->cfg.dim == 3 && h->cfg.grid_every && h->mc.nodes &&
-                                 h->step_index % h->cfg.grid_every == 0;
         int rc;
-        if (h->persistent && !h->profiling && !surface_due) {
-            rc = h->cfg.dim == 3 ? run_step_persistent<3>(h) : run_step_persistent<2>(h);
-        } else if (h->use_graph && !h->profiling && !surface_due) {
+        if (h->persistent && !h->profiling && !surface_due(h->step_index)) {
+            // the steps up to the next surface step in one launch (one at a
+            // time while splits can grow the count)
+            int run = 1;
+            if (!h->cfg.use_split)
+                while (run < nsteps - k && run < kPersistMaxSteps && !surface_due(h->step_index + run)) ++run;
+            if (run > 1 && h->rb_pending[h->cur]) {   // it writes both state buffers
+                cudaStreamWaitEvent(h->stream, h->rb_done[h->cur], 0);
+                h->rb_pending[h->cur] = false;
+            }
+            rc = h->cfg.dim == 3 ? run_step_persistent<3>(h, run) : run_step_persistent<2>(h, run);
+            k += run - 1;
+        } else if (h->use_graph && !h->profiling && !surface_due(h->step_index)) {
             const int p = h->cur;
             if (!h->graph[p] || h->graph_grid[p] != launch_key(h)) {
                 rc = capture_step(h);

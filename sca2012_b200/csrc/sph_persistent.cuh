@@ -17,7 +17,8 @@
 // (the bracketed stages only when split or merge is on): 13 barriers per step
 // with adaptivity.  Without it the write-out runs in the energy stage and
 // hashes the next step's state too (write_hash_by_slot_body), so the next
-// launch starts at the scan: 6 barriers per step.  Each scan's second phase has every block sum
+// step starts at the scan: 6 barriers per step.  One launch runs several
+// steps, one more barrier between two of them.  Each scan's second phase has every block sum
 // the block totals itself (scan_phase23_body) instead of one block scanning
 // them between two barriers.  Every particle's
 // arithmetic is the ordinary path's, in the same order, so the results are
@@ -65,6 +66,8 @@ struct PersistArgs {
     int ranks;               // split or merge on: run the split and removal scans
     int cluster;             // the grid is one thread-block cluster: hardware cluster barriers
     int hash_ready;          // the previous launch hashed this step's state already
+    int parity;              // the state buffer (and counters) the first step reads
+    int nsteps;              // steps this launch runs
 };
 
 // Without split and merge (ranks = 0) the write-out needs no global step:
@@ -186,66 +189,100 @@ __device__ __forceinline__ bool grid_scan(const PersistArgs &a, uint32_t &k, Cou
     return true;
 }
 
+// Cell scans of at most this many cells per thread of a block run in one
+// phase (scan_onepass_body): each block reads every count before its chunk.
+constexpr uint32_t kOnePassPerThread = 16;
+
+// One step's stages, from the hash (or, when the previous step hashed this
+// state already, from the cell scan) to the write-out.  Returns false, for
+// the whole block, once any block has given up at a barrier.
 template <int DIM, int BS>
-__global__ void __launch_bounds__(BS, 2) k_step_persistent(sph_config c, Counters *cin, Counters *cout, CanonPtrs in,
-                                                        CanonPtrs out, WorkPtrs w, PersistArgs a)
+__device__ __forceinline__ bool step_stages(const sph_config &c, Counters *cin, Counters *cout, const CanonPtrs &in,
+                                            const CanonPtrs &out, const WorkPtrs &w, const PersistArgs &a,
+                                            uint32_t &k, bool hashed, WarpPairSmem *pair, MergeSmem *merge)
+{
+    if (!a.ranks && blockIdx.x == 0 && threadIdx.x == 0) {
+        cin->n_split = 0u;
+        cin->n_removed = 0u;
+        cin->split_off = 0u;
+    }
+    if (!hashed) {
+        hash_body<DIM>(c, cin, in, w);
+        if (!grid_barrier(a, ++k, cin, cout)) return false;
+    }
+    if (a.ncells <= kOnePassPerThread * blockDim.x) {   // few cells: one phase, one barrier fewer
+        scan_onepass_body<uint32_t, kOnePassPerThread>(w.cell_count, w.cell_off, a.ncells, a.scan_grand, 1);
+    } else if (!grid_scan<uint32_t>(a, k, cin, cout, w.cell_count, w.cell_off, a.ncells, a.scan_grand, 1,
+                                    nullptr)) {
+        return false;
+    }
+    if (!grid_barrier(a, ++k, cin, cout)) return false;
+    scatter_body<false>(cin, w);
+    // no stage reads the counts after the scan: clear them for the next hash
+    for (uint32_t q = grid_stride_start(); q < a.ncells; q += grid_stride()) w.cell_count[q] = 0u;
+    if (!grid_barrier(a, ++k, cin, cout)) return false;
+    reorder_body<false>(cin, in, w);
+    if (!grid_barrier(a, ++k, cin, cout)) return false;
+    density_body<DIM, false>(c, cin, w);
+    if (!grid_barrier(a, ++k, cin, cout)) return false;
+    force_integrate_body<DIM, BS, false>(c, cin, w, pair);
+    if (!grid_barrier(a, ++k, cin, cout)) return false;
+    energy_split_body<DIM, BS, false>(c, cin, in, w, a.want_tv, pair);
+    if (!a.ranks) {
+        write_hash_by_slot_body<DIM, BS>(c, cin, cout, in, out, w);
+        return true;
+    }
+    if (!grid_barrier(a, ++k, cin, cout)) return false;
+    const uint32_t n = cin->n;
+    if (!grid_scan<uint32_t>(a, k, cin, cout, w.split_c, w.split_rank, n, &cin->n_split, 0, w.split_list))
+        return false;
+    if (blockIdx.x == 0 && threadIdx.x == 0) split_guard_body(c, cin, a.cap);
+    if (!grid_barrier(a, ++k, cin, cout)) return false;
+    if (c.use_merge) {
+        if (c.merge_rule == SPH_MERGE_SIBLING) merge_sibling_body<DIM>(c, cin, in, w);
+        else merge_body<DIM>(c, cin, in, w, a.ncells, a.cap, merge);
+        if (!grid_barrier(a, ++k, cin, cout)) return false;
+    }
+    if (!grid_scan<uint32_t>(a, k, cin, cout, w.removed_c, w.removed_rank, n, &cin->n_removed, 0, nullptr))
+        return false;
+    if (!grid_barrier(a, ++k, cin, cout)) return false;
+    write_body<DIM>(c, cin, cout, in, out, w, true);
+    return true;
+}
+
+// a.nsteps steps from state buffer a.parity (buf.b[parity], cnt[parity]);
+// step j reads buffer (parity + j) & 1 and writes the other, as that many
+// separate steps would.  A barrier separates one step's write-out from the
+// next step's first stage.
+struct CanonPair {
+    CanonPtrs b[2];
+};
+
+template <int DIM, int BS>
+__global__ void __launch_bounds__(BS, 2) k_step_persistent(sph_config c, Counters *cnt,
+                                                        const __grid_constant__ CanonPair buf, WorkPtrs w,
+                                                        PersistArgs a)
 {
     // one shared buffer for the stages that use shared memory
     __shared__ union {
         WarpPairSmem pair[BS / 32];
         MergeSmem merge[BS / 32];
     } sm;
-    if (cin->error & (1u << SPH_ERR_TIMEOUT)) {   // a step before gave up: nothing to step from
-        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&cout->error, cin->error);
+    const int p = a.parity;
+    if (cnt[p].error & (1u << SPH_ERR_TIMEOUT)) {   // a step before gave up: nothing to step from
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&cnt[p ^ 1].error, cnt[p].error);
         return;
     }
-    // the cell counts are zero here: the previous persistent step's write-out
-    // cleared them, and the host clears them after any other step
-    uint32_t k = 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) *a.gs_next = GridSync{0u, 0u, 0u, 0u};
-    if (!a.ranks && blockIdx.x == 0 && threadIdx.x == 0) {
-        cin->n_split = 0u;
-        cin->n_removed = 0u;
-        cin->split_off = 0u;
-    }
-    if (!a.hash_ready) {
-        hash_body<DIM>(c, cin, in, w);
-        if (!grid_barrier(a, ++k, cin, cout)) return;
-    }
-    if (!grid_scan<uint32_t>(a, k, cin, cout, w.cell_count, w.cell_off, a.ncells, a.scan_grand, 1, nullptr)) return;
-    if (!grid_barrier(a, ++k, cin, cout)) return;
-    scatter_body<false>(cin, w);
-    // no stage reads the counts after the scan: clear them for the next hash
-    for (uint32_t q = grid_stride_start(); q < a.ncells; q += grid_stride()) w.cell_count[q] = 0u;
-    if (!grid_barrier(a, ++k, cin, cout)) return;
-    reorder_body<false>(cin, in, w);
-    if (!grid_barrier(a, ++k, cin, cout)) return;
-    density_body<DIM, false>(c, cin, w);
-    if (!grid_barrier(a, ++k, cin, cout)) return;
-    force_integrate_body<DIM, BS, false>(c, cin, w, sm.pair);
-    if (!grid_barrier(a, ++k, cin, cout)) return;
-    energy_split_body<DIM, BS, false>(c, cin, in, w, a.want_tv, sm.pair);
-    if (!a.ranks) {
-        write_hash_by_slot_body<DIM, BS>(c, cin, cout, in, out, w);
-        return;
-    }
-    if (!grid_barrier(a, ++k, cin, cout)) return;
-    {
-        const uint32_t n = cin->n;
-        if (!grid_scan<uint32_t>(a, k, cin, cout, w.split_c, w.split_rank, n, &cin->n_split, 0, w.split_list))
+    uint32_t k = 0;
+    for (int j = 0; j < a.nsteps; ++j) {
+        const int q = (p + j) & 1;
+        Counters *cin = cnt + q, *cout = cnt + (q ^ 1);
+        if (j > 0 && !grid_barrier(a, ++k, cin, cout)) return;
+        const bool hashed = j > 0 ? !a.ranks : a.hash_ready != 0;
+        if (!step_stages<DIM, BS>(c, cin, cout, buf.b[q], buf.b[q ^ 1], w, a, k, hashed, sm.pair, sm.merge))
             return;
-        if (blockIdx.x == 0 && threadIdx.x == 0) split_guard_body(c, cin, a.cap);
-        if (!grid_barrier(a, ++k, cin, cout)) return;
-        if (c.use_merge) {
-            if (c.merge_rule == SPH_MERGE_SIBLING) merge_sibling_body<DIM>(c, cin, in, w);
-            else merge_body<DIM>(c, cin, in, w, a.ncells, a.cap, sm.merge);
-            if (!grid_barrier(a, ++k, cin, cout)) return;
-        }
-        if (!grid_scan<uint32_t>(a, k, cin, cout, w.removed_c, w.removed_rank, n, &cin->n_removed, 0, nullptr))
-            return;
-        if (!grid_barrier(a, ++k, cin, cout)) return;
     }
-    write_body<DIM>(c, cin, cout, in, out, w, true);
 }
 
 }  // namespace sph

@@ -198,6 +198,43 @@ __device__ __forceinline__ void scan_phase23_body(const T *in, T *out, uint32_t 
     if (out_total_at_len && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[len] = total;
 }
 
+// The whole scan in one phase, for inputs of at most PER elements per
+// thread of one block (len <= PER * blockDim.x): every block sums all the
+// elements before its chunk itself (PER independent loads per thread, in
+// flight together), so no barrier separates the block totals from the
+// rescan.  The last block (whose chunk ends at len) writes the grand total to
+// *grand (if non-null) and, if out_total_at_len, to out[len].
+template <typename T, int PER>
+__device__ __forceinline__ void scan_onepass_body(const T *in, T *out, uint32_t len, T *grand, int out_total_at_len)
+{
+    __shared__ T wt[kScanThreads / 32];
+    uint32_t b, e;
+    chunk_of(len, b, e);
+    T part[PER];
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+        const uint32_t i = threadIdx.x + (uint32_t)u * blockDim.x;
+        part[u] = i < b ? in[i] : zero_of<T>();
+    }
+    T pre = zero_of<T>();
+#pragma unroll
+    for (int u = 0; u < PER; ++u) pre = pre + part[u];
+    T carry;
+    block_inclusive_scan(pre, wt, &carry);
+    for (uint32_t base = b; base < e; base += blockDim.x) {
+        uint32_t i = base + threadIdx.x;
+        T v = i < e ? in[i] : zero_of<T>();
+        T t2;
+        T inc = block_inclusive_scan(v, wt, &t2);
+        if (i < e) out[i] = carry + inc - v;
+        carry = carry + t2;
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
+        if (grand) *grand = carry;
+        if (out_total_at_len) out[len] = carry;
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kScanThreads) scan_phase3(const T *__restrict__ in, T *__restrict__ out,
                                                            const uint32_t *len_ptr, uint32_t len_const,
