@@ -1114,12 +1114,17 @@ int sph_read_particles_async(sph_handle *h, void *mapped_dst, uint64_t capacity_
         cudaEventCreateWithFlags(&h->rb_done[0], cudaEventDisableTiming);
         cudaEventCreateWithFlags(&h->rb_done[1], cudaEventDisableTiming);
     }
+    if ((reinterpret_cast<uintptr_t>(dst_dev) | reinterpret_cast<uintptr_t>(cnt_dev)) & 3u) {
+        h->err = "sph_read_particles_async: destination and count need 4-byte alignment";
+        return SPH_ERR_INVALID;
+    }
     const int p = h->cur;
     const uint64_t rec = sph_particle_record_size(h);
     const uint32_t max_rec = (uint32_t)std::min<uint64_t>(capacity_bytes / rec, h->cap);
     cudaEventRecord(h->rb_ready, h->stream);
     cudaStreamWaitEvent(h->rb_stream, h->rb_ready, 0);
-    const uint32_t G = grid_for(h, h->n_ub);
+    // a few blocks keep PCIe busy; the rest of the GPU stays with the next step
+    const uint32_t G = std::min<uint32_t>(grid_for(h, h->n_ub), (uint32_t)std::max(1, h->num_sms / 4));
     if (h->cfg.dim == 3)
         k_to_aos_mapped<3><<<G, kThreads, 0, h->rb_stream>>>(h->cnt + p, h->buf[p], (float *)dst_dev, max_rec,
                                                              (uint32_t *)cnt_dev);

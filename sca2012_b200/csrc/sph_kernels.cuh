@@ -1253,28 +1253,41 @@ __global__ void __launch_bounds__(kThreads) k_to_aos(const Counters *__restrict_
 }
 
 // Same records written straight into mapped page-locked host memory (at most
-// max_rec of them) plus the live count; a warp's stores are contiguous.
+// max_rec of them) plus the live count.  Each block builds 256 records in
+// shared memory and then stores them as one contiguous run, a warp writing
+// 128 consecutive bytes per store, so the writes cross PCIe as full lines
+// (a thread storing its own record would scatter 4-byte writes 72 bytes
+// apart).  dst needs 4-byte alignment only.
 template <int DIM>
 __global__ void __launch_bounds__(kThreads) k_to_aos_mapped(const Counters *__restrict__ cnt, CanonPtrs st,
                                                            float *dst, uint32_t max_rec, uint32_t *count_dst)
 {
+    constexpr int W = AosLayout<DIM>::words;
+    __shared__ float stage[kThreads * W];
     const uint32_t n = cnt->n;
     const uint32_t m = min(n, max_rec);
-    constexpr int W = AosLayout<DIM>::words;
     if (blockIdx.x == 0 && threadIdx.x == 0) *count_dst = n;
-    for (uint32_t i = grid_stride_start(); i < m; i += grid_stride()) {
-        const float4 p = st.pos[i], v = st.vel[i], e = st.ev[i], a = st.acc[i];
-        float *o = dst + (size_t)i * W;
-        if (DIM == 3) {
-            o[0] = p.x; o[1] = p.y; o[2] = p.z; o[3] = v.x; o[4] = v.y; o[5] = v.z;
-            o[6] = e.x; o[7] = e.y; o[8] = e.z; o[9] = a.x; o[10] = a.y; o[11] = a.z;
-            o[12] = st.dens[i]; o[13] = st.press[i]; o[14] = st.energy[i]; o[15] = st.surface[i];
-            o[16] = 0.0f; o[17] = __uint_as_float((uint32_t)p.w);
-        } else {
-            o[0] = p.x; o[1] = p.y; o[2] = v.x; o[3] = v.y; o[4] = e.x; o[5] = e.y; o[6] = a.x; o[7] = a.y;
-            o[8] = st.dens[i]; o[9] = st.press[i]; o[10] = st.energy[i];
-            o[11] = __uint_as_float((uint32_t)p.w); o[12] = st.surface[i]; o[13] = 0.0f;
+    for (uint32_t base = blockIdx.x * kThreads; base < m; base += gridDim.x * kThreads) {
+        const uint32_t i = base + threadIdx.x;
+        if (i < m) {
+            const float4 p = st.pos[i], v = st.vel[i], e = st.ev[i], a = st.acc[i];
+            float *o = stage + threadIdx.x * W;
+            if (DIM == 3) {
+                o[0] = p.x; o[1] = p.y; o[2] = p.z; o[3] = v.x; o[4] = v.y; o[5] = v.z;
+                o[6] = e.x; o[7] = e.y; o[8] = e.z; o[9] = a.x; o[10] = a.y; o[11] = a.z;
+                o[12] = st.dens[i]; o[13] = st.press[i]; o[14] = st.energy[i]; o[15] = st.surface[i];
+                o[16] = 0.0f; o[17] = __uint_as_float((uint32_t)p.w);
+            } else {
+                o[0] = p.x; o[1] = p.y; o[2] = v.x; o[3] = v.y; o[4] = e.x; o[5] = e.y; o[6] = a.x; o[7] = a.y;
+                o[8] = st.dens[i]; o[9] = st.press[i]; o[10] = st.energy[i];
+                o[11] = __uint_as_float((uint32_t)p.w); o[12] = st.surface[i]; o[13] = 0.0f;
+            }
         }
+        __syncthreads();
+        const uint32_t words = min((uint32_t)kThreads, m - base) * W;
+        float *out = dst + (size_t)base * W;
+        for (uint32_t q = threadIdx.x; q < words; q += kThreads) out[q] = stage[q];
+        __syncthreads();   // the stage is refilled next round
     }
 }
 
