@@ -9,7 +9,7 @@
 // sph_scan.cuh) in one launch whose blocks are all resident (a cooperative
 // launch), separated by grid-wide barriers:
 //
-//   hash | scan cells (2 phases) | scatter (and clear the counts) | reorder |
+//   hash | scan cells (1 or 2 phases) | scatter (and clear the counts) | reorder |
 //   density | force + integrate | energy + split decision |
 //   [split scan (2 phases) + capacity guard | merge | removal scan (2 phases)] |
 //   write-out
@@ -17,8 +17,9 @@
 // (the bracketed stages only when split or merge is on): 13 barriers per step
 // with adaptivity.  Without it the write-out runs in the energy stage and
 // hashes the next step's state too (write_hash_by_slot_body), so the next
-// step starts at the scan: 6 barriers per step.  One launch runs several
-// steps, one more barrier between two of them.  Each scan's second phase has every block sum
+// step starts at the scan, and a small cell grid is scanned in one phase:
+// 5 barriers per step.  One launch runs several steps without splits, one
+// more barrier between two of them.  Each scan's second phase has every block sum
 // the block totals itself (scan_phase23_body) instead of one block scanning
 // them between two barriers.  Every particle's
 // arithmetic is the ordinary path's, in the same order, so the results are

@@ -44,8 +44,9 @@ def main():
     ap.add_argument("--bpsm", default="")
     ap.add_argument("--regcap", default="")
     ap.add_argument("--workload", default="dam_3d4", choices=["dam_3d4", "dam_2d"],
-                    help="dam_2d: the 4,096-particle 2D dam (no adaptivity)")
-    ap.add_argument("--persistent", action="store_true", help="run each step as one persistent launch")
+                    help="dam_2d: the 4,096-particle 2D dam (no adaptivity), stepped K steps twice")
+    ap.add_argument("--persistent", action="store_true",
+                    help="persistent launches (dam_2d: one launch per K steps; dam_3d4: one per step)")
     a = ap.parse_args()
     if a.workload == "dam_2d":
         cfg = sph.preset(sph.PRESET_DAM_2D)
@@ -53,10 +54,11 @@ def main():
         s = sph.Solver(cfg)
         s.set_persistent(a.persistent)
         s.set_state(dict(pos=pos, vel=vel, level=lvl))
-        s.step(a.steps)
+        for _ in range(2):   # persistent: two launches of K steps each (K <= 256)
+            s.step(a.steps)
         rc = s.sync_status()
         s.close()
-        print(f"profile_case: 2D dam, {a.steps} steps, persistent {a.persistent}, status {rc}")
+        print(f"profile_case: 2D dam, 2 x {a.steps} steps, persistent {a.persistent}, status {rc}")
         return 0 if rc == 0 else 1
     cfg = sph.preset(sph.PRESET_DAM_3D4)
     pos, vel, lvl = scenes.dam_3d4(cfg)
