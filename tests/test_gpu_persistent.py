@@ -211,3 +211,44 @@ def test_persistent_multi_step_launch_waits_for_readbacks(gpu):
         n = int(cnts[j].numpy().view(np.uint32)[0])
         assert n == len(want[j])
         assert bufs[j].numpy()[: n * rec].tobytes() == want[j].tobytes(), f"readback {j} differs"
+
+
+def test_persistent_runs_break_at_surface_steps(gpu):
+    """Plain 3D steps with a density grid and marching cubes every 5 steps:
+    the persistent launches stop before each surface step (which runs the
+    ordinary launches) and resume after it; state and the last mesh equal the
+    ordinary path's."""
+    import ctypes as C
+    cfg = sph.preset(sph.PRESET_DAM_3D2)
+    pos, vel, lvl = scenes.block_3d(cfg, (20, 20, 10), 0.01, seed=3)
+    cfg.use_split = cfg.use_merge = 0
+    cfg.grid_every = 5
+    cfg.max_particle = 4 * len(pos)
+    G = int(np.prod([cfg.ndens[a] for a in range(3)]))
+    mx = min(3 * G, int(cfg.max_triangles)) if cfg.max_triangles else 3 * G
+
+    def run(persistent):
+        s = sph.Solver(cfg)
+        s.set_state(dict(pos=pos, vel=vel, level=lvl))
+        s.set_persistent(persistent)
+        s.step(23)   # surface steps 0, 5, 10, 15, 20
+        assert s.sync_status() == 0
+        launches = s.last_launch_count()
+        bufs = [np.zeros((mx, 3), np.float32) for _ in range(6)]
+        mv = sph.MeshView()
+        mv.max_triangles = mx
+        for k, b in zip(("v0", "v1", "v2", "n0", "n1", "n2"), bufs):
+            setattr(mv, k, b.ctypes.data_as(C.POINTER(C.c_float)))
+        assert s._lib.sph_extract_surface(s._h, C.byref(mv)) == 0
+        nt = int(mv.num_triangles)
+        mesh = np.stack([b[:nt] for b in bufs], 1)
+        st = s.get_state()
+        s.close()
+        return st, mesh, launches
+
+    a, ma, la = run(False)
+    b, mb, lb = run(True)
+    for f in FIELDS:
+        assert _same(a[f], b[f]), f
+    assert len(ma) > 100 and _same(ma, mb)
+    assert lb < la
