@@ -421,7 +421,7 @@ __device__ __forceinline__ float4 node_pos(const LossGrid &g, uint32_t a, uint32
 // residual G - target, and sum of squared residuals (FP64).
 template <int DIM>
 __global__ void __launch_bounds__(kThreads) k_loss_grid(sph_config c, WorkPtrs w, LossGrid g, const float *target,
-                                                        float *grid, float *resid, double *sum)
+                                                        float *grid, float *resid)
 {
     const uint32_t N = g.n[0] * g.n[1] * (DIM == 3 ? g.n[2] : 1u);
     for (uint32_t id = grid_stride_start(); id < N; id += grid_stride()) {
@@ -448,11 +448,39 @@ __global__ void __launch_bounds__(kThreads) k_loss_grid(sph_config c, WorkPtrs w
                 }
             }
         grid[id] = G;
-        const float R = G - target[id];
-        resid[id] = R;
-        const double r2d = (double)R * (double)R;
-        add_param(sum, 0u, r2d, 0.0);
+        resid[id] = G - target[id];
     }
+}
+
+// The loss's FP64 sum of squares of the residuals x[0, n), the same bits on
+// every run: each block sums its grid-stride share and tree-reduces it in a
+// fixed order into part[block]; k_sum_blocks adds the partials in block order.
+// (Atomic adds would sum in arrival order, which varies between runs.)
+constexpr uint32_t kLossPartials = 4096;
+
+__global__ void __launch_bounds__(kThreads) k_sumsq_blocks(const float *__restrict__ x, uint32_t n, double *part)
+{
+    __shared__ double sh[kThreads];
+    double acc = 0.0;
+    for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) {
+        const double v = (double)x[i];
+        acc += v * v;
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (uint32_t off = kThreads / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) sh[threadIdx.x] += sh[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void k_sum_blocks(const double *__restrict__ part, uint32_t nb, double *out)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double t = 0.0;
+    for (uint32_t b = 0; b < nb; ++b) t += part[b];
+    *out = t;
 }
 
 // Adjoint of mean((G - target)^2) with respect to the canonical positions.

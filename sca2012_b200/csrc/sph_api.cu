@@ -201,10 +201,9 @@ void scan_u32(sph_handle *h, const uint32_t *in, uint32_t *out, const uint32_t *
               uint32_t *grand, int total_at_len, uint32_t *list)
 {
     scan_phase1<uint32_t><<<kScanBlocks, kScanThreads, 0, h->stream>>>(in, len_ptr, len_const, h->scan_blocks);
-    scan_phase2<uint32_t><<<1, kScanBlocks, 0, h->stream>>>(h->scan_blocks, grand);
-    scan_phase3<uint32_t><<<kScanBlocks, kScanThreads, 0, h->stream>>>(in, out, len_ptr, len_const, h->scan_blocks,
-                                                                       grand, total_at_len, list);
-    h->last_launches += 3;
+    scan_phase23<uint32_t><<<kScanBlocks, kScanThreads, 0, h->stream>>>(in, out, len_ptr, len_const, h->scan_blocks,
+                                                                        grand, total_at_len, list);
+    h->last_launches += 2;
 }
 
 // Marching cubes over the current device grid: classify, scan, emit.

@@ -417,7 +417,7 @@ int sph_rollout_forward(sph_handle *h, uint32_t nsteps, uint32_t every)
         rc |= ralloc(h, r, &r->gx2, r->cap); rc |= ralloc(h, r, &r->gv2, r->cap); rc |= ralloc(h, r, &r->gev2, r->cap);
         rc |= ralloc(h, r, &r->gxd, r->cap); rc |= ralloc(h, r, &r->gf, r->cap); rc |= ralloc(h, r, &r->gevd, r->cap);
         rc |= ralloc(h, r, &r->grho, r->cap);
-        rc |= ralloc(h, r, &r->lsum, 2);
+        rc |= ralloc(h, r, &r->lsum, 2 + kLossPartials);
         if (rc) {
             rollout_free(r);
             h->ro = nullptr;
@@ -460,7 +460,7 @@ int sph_splat_loss(sph_handle *h, const sph_loss_grid *g, const float *target, f
         Rollout *r = h->ro = new Rollout();
         r->cap = h->cap;
         r->ncells = h->ncells;
-        if (ralloc(h, r, &r->lsum, 2)) { rollout_free(r); h->ro = nullptr; return SPH_ERR_CUDA; }
+        if (ralloc(h, r, &r->lsum, 2 + kLossPartials)) { rollout_free(r); h->ro = nullptr; return SPH_ERR_CUDA; }
     }
     Rollout *r = h->ro;
     if (N > r->node_cap) {
@@ -478,15 +478,17 @@ int sph_splat_loss(sph_handle *h, const sph_loss_grid *g, const float *target, f
     r->grid.spacing = g->spacing;
     cudaStream_t s = h->stream;
     cudaMemcpyAsync(r->target, target, sizeof(float) * N, cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(r->lsum, 0, 2 * sizeof(double), s);
     const uint32_t G = grid_for(h, (uint32_t)N);
     if (dim == 3) {
         sort_only<3>(h);
-        k_loss_grid<3><<<G, kThreads, 0, s>>>(h->cfg, h->w, r->grid, r->target, r->gridv, r->resid, r->lsum);
+        k_loss_grid<3><<<G, kThreads, 0, s>>>(h->cfg, h->w, r->grid, r->target, r->gridv, r->resid);
     } else {
         sort_only<2>(h);
-        k_loss_grid<2><<<G, kThreads, 0, s>>>(h->cfg, h->w, r->grid, r->target, r->gridv, r->resid, r->lsum);
+        k_loss_grid<2><<<G, kThreads, 0, s>>>(h->cfg, h->w, r->grid, r->target, r->gridv, r->resid);
     }
+    const uint32_t GL = std::min<uint32_t>(G, kLossPartials);
+    k_sumsq_blocks<<<GL, kThreads, 0, s>>>(r->resid, (uint32_t)N, r->lsum + 2);
+    k_sum_blocks<<<1, 1, 0, s>>>(r->lsum + 2, GL, r->lsum);
     double sum = 0.0;
     cudaMemcpyAsync(&sum, r->lsum, sizeof(double), cudaMemcpyDeviceToHost, s);
     if (grid_out) cudaMemcpyAsync(grid_out, r->gridv, sizeof(float) * N, cudaMemcpyDeviceToHost, s);

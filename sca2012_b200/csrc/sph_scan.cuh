@@ -3,10 +3,12 @@
 // never needs the host to learn the count (the reference syncs on two
 // thrust::reduce calls per step, SPH-3D-2/sph_system.cu:1639,1836).
 //
-// Three launches: per-block chunk totals, one block scanning the totals,
-// per-block rescans with the block offset.  The grid is fixed at launch
-// (kScanBlocks); each block takes a contiguous chunk of ceil(len/kScanBlocks)
-// elements, so the traffic is two reads and one write of the input.
+// Two launches: per-block chunk totals, then per-block rescans, each block
+// summing the block totals before its own (scan_phase23).  The grid is fixed
+// at launch (kScanBlocks); each block takes a contiguous chunk of
+// ceil(len/kScanBlocks) elements, so the traffic is two reads and one write
+// of the input.  (The three-launch form, with one block scanning the totals
+// in between, remains for the no-allocation sort.)
 #pragma once
 #include <cstdint>
 
@@ -233,6 +235,16 @@ __device__ __forceinline__ void scan_onepass_body(const T *in, T *out, uint32_t 
         if (grand) *grand = carry;
         if (out_total_at_len) out[len] = carry;
     }
+}
+
+// Phases 2 and 3 as one launch (after scan_phase1 over the same grid).
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) scan_phase23(const T *__restrict__ in, T *__restrict__ out,
+                                                            const uint32_t *len_ptr, uint32_t len_const,
+                                                            const T *__restrict__ block_tot, T *grand,
+                                                            int out_total_at_len, uint32_t *list)
+{
+    scan_phase23_body<T>(in, out, len_ptr ? *len_ptr : len_const, block_tot, grand, out_total_at_len, list);
 }
 
 template <typename T>
