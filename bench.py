@@ -49,13 +49,15 @@ WORKLOAD = ("dam_3d4: 1,048,576-particle block (s=0.005) + 65,536-particle spher
 # Algorithmic (compulsory) bytes per particle of each stage, every array read
 # or written once (neighbour data re-reads are cache traffic, not counted).
 STAGE_BYTES = {
-    "hash": 16 + 4 + 4 + 4,                  # pos in; key, slot out; count atomics
+    "hash": 16 + 4 + 4 + 4,                  # pos in; key, slot out; count atomics (only a state no
+                                             # step wrote: the write-out hashes the next state)
     "scatter": 4 + 4 + 4 + 4,                # key, slot, offset in; index out
     "reorder": 4 + 4 + 48 + 4 + 4 + 4,       # index, key, pos/vel/ev in; sidx, skey, inv out
     "density": 16 + 4 + 8,                   # pos, m in; rho, p out (the unfused figure per stage)
     "force_integrate": 16 * 4 + 16 * 4 + 4,  # pos, ev, aux, vel in; pos, vel, ev, acc, surface out
     "energy_split": 16 + 16 + 4 + 16 + 4 + 4 + 4 + 4 + 4,  # new pos, vel, surf, aux, nbr, idx; energy, flags
-    "write": 4 * 16 + 16 + 4 * 4 + 4 * 4 + 4 * 16 + 5 * 4,  # sorted state + flags in; canonical state out
+    "write": 4 * 16 + 16 + 4 * 4 + 4 * 4 + 4 * 16 + 5 * 4 + 4 + 4,  # sorted state + flags in; canonical state,
+                                                                        # next step's key and slot out
 }
 
 

@@ -226,7 +226,31 @@ void stage(sph_handle *h, const char *name)
     cudaEventRecord(h->ev[++h->nstages], h->stream);
 }
 
-template <int DIM> int run_step(sph_handle *h)
+// The cell counts, keys and slots hold the hash of the current state: the
+// step that wrote it hashed it (its write-out), and nothing has changed the
+// state, the config or the counts since.
+static bool hash_ready(const sph_handle *h)
+{
+    return h->counts_hashed && h->hashed_gen == h->state_gen && h->hashed_step == h->step_index;
+}
+
+// Clears the cell counts and hashes the current state (the first stage of a
+// step whose state no step has hashed).
+template <int DIM> void hash_prologue(sph_handle *h)
+{
+    const sph_config &c = h->cfg;
+    const int p = h->cur;
+    WorkPtrs w = h->w;
+    cudaStream_t s = h->stream;
+    cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, s);
+    SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_HASH],
+                  k_hash<DIM, B><<<grid_st(h, h->n_ub, SPH_TUNE_HASH), B, 0, s>>>(c, h->cnt + p, h->buf[p], w));
+    h->last_launches += 1;
+}
+
+// One step as separate launches.  prologue = false leaves out the hash of a
+// state no step has hashed (a captured graph: the replay runs it when needed).
+template <int DIM> int run_step(sph_handle *h, bool prologue = true)
 {
     const sph_config &c = h->cfg;
     const int p = h->cur;
@@ -241,14 +265,15 @@ template <int DIM> int run_step(sph_handle *h)
     h->nstages = 0;
     if (h->profiling) cudaEventRecord(h->ev[0], s);
 
-    cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, s);
-    h->counts_zero = false;   // this step leaves its counts behind
-    h->counts_hashed = false;
     const uint32_t nub = h->n_ub;
-    SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_HASH],
-                  k_hash<DIM, B><<<grid_st(h, nub, SPH_TUNE_HASH), B, 0, s>>>(c, cin, in, w));
-    stage(h, "hash");
+    if (prologue && !hash_ready(h)) {
+        hash_prologue<DIM>(h);
+        stage(h, "hash");
+    }
     scan_u32(h, w.cell_count, w.cell_off, nullptr, h->ncells, h->scan_grand, 1, nullptr);
+    // the scan has read the counts: cleared for the write-out's hash of the next state
+    cudaMemsetAsync(w.cell_count, 0, sizeof(uint32_t) * h->ncells, s);
+    h->counts_zero = false;
     stage(h, "scan_cells");
     SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_SCATTER], k_scatter<B><<<grid_st(h, nub, SPH_TUNE_SCATTER), B, 0, s>>>(cin, w));
     stage(h, "scatter");
@@ -294,11 +319,14 @@ template <int DIM> int run_step(sph_handle *h)
     scan_u32(h, w.removed_c, w.removed_rank, &cin->n, 0, &cin->n_removed, 0, nullptr);
     stage(h, "scan_removed");
     SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_WRITE],
-                  k_write<DIM, B><<<grid_st(h, nub, SPH_TUNE_WRITE), B, 0, s>>>(c, cin, cout, in, out, w));
+                  k_write<DIM, B><<<grid_st(h, nub, SPH_TUNE_WRITE), B, 0, s>>>(c, cin, cout, in, out, w, 1));
     h->last_launches += 1;
     stage(h, "write");
     h->cur = p ^ 1;
     h->step_index++;
+    h->counts_hashed = true;   // the write-out hashed the new state
+    h->hashed_gen = h->state_gen;
+    h->hashed_step = h->step_index;
     uint64_t ub = h->n_ub;
     if (c.use_split) ub *= (c.split_ways == 4 ? 4u : 2u);
     h->n_ub = (uint32_t)std::min<uint64_t>(ub, h->cap);
@@ -317,11 +345,6 @@ constexpr uint32_t kPersistMaxBlocks = 1024;
 // A grid of at most kPersistMaxCluster blocks of 256 threads is launched as
 // one cluster when the device can hold it; -1 in cluster_ok: it cannot.
 constexpr uint32_t kPersistMaxCluster = 16;
-
-static bool hash_ready(const sph_handle *h)
-{
-    return h->counts_hashed && h->hashed_gen == h->state_gen && h->hashed_step == h->step_index;
-}
 
 template <int DIM> int launch_persistent_cluster(sph_handle *h, int &cluster_ok, uint32_t G, int nsteps)
 {
@@ -438,11 +461,10 @@ template <int DIM> int run_step_persistent(sph_handle *h, int nsteps)
         if (rc) return rc;
         h->persist_launch++;   // the polled barriers alternate between their two states
     }
-    // the scatter stage cleared the counts; without split and merge the
-    // write-out then hashed the new state into them
-    const bool plain = !(c.use_split || c.use_merge);
-    h->counts_zero = !plain;
-    h->counts_hashed = plain;
+    // the scatter stage cleared the counts and the write-out hashed the new
+    // state into them
+    h->counts_zero = false;
+    h->counts_hashed = true;
     h->last_launches += 1;
     h->cur = (p + nsteps) & 1;
     h->step_index += (uint64_t)nsteps;
@@ -745,17 +767,23 @@ static int capture_step(sph_handle *h)
     const int p = h->cur;
     const uint64_t step_index = h->step_index;
     const uint32_t n_ub = h->n_ub, launches = h->last_launches;
+    const bool counts_zero = h->counts_zero, counts_hashed = h->counts_hashed;
+    const uint64_t hashed_gen = h->hashed_gen, hashed_step = h->hashed_step;
     cudaGraph_t g = nullptr;
     h->last_launches = 0;
     if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
         return cuda_check(h, "cudaStreamBeginCapture");
-    int rc = h->cfg.dim == 3 ? run_step<3>(h) : run_step<2>(h);
+    int rc = h->cfg.dim == 3 ? run_step<3>(h, false) : run_step<2>(h, false);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     h->graph_launches[p] = h->last_launches;
     h->cur = p;
     h->step_index = step_index;
     h->n_ub = n_ub;
     h->last_launches = launches;
+    h->counts_zero = counts_zero;
+    h->counts_hashed = counts_hashed;
+    h->hashed_gen = hashed_gen;
+    h->hashed_step = hashed_step;
     if (rc) return rc;
     if (e != cudaSuccess) return cuda_check(h, "cudaStreamEndCapture");
     if (h->graph[p]) cudaGraphExecDestroy(h->graph[p]);
@@ -801,12 +829,18 @@ int sph_step(sph_handle *h, int nsteps)
                 rc = capture_step(h);
                 if (rc) return rc;
             }
+            if (!hash_ready(h)) {   // the graph starts at the cell scan
+                if (h->cfg.dim == 3) hash_prologue<3>(h);
+                else hash_prologue<2>(h);
+            }
             if (cudaGraphLaunch(h->graph[p], h->stream) != cudaSuccess) return cuda_check(h, "cudaGraphLaunch");
             // the bookkeeping run_step does on the host
             h->counts_zero = false;
-            h->counts_hashed = false;
             h->cur = p ^ 1;
             h->step_index++;
+            h->counts_hashed = true;
+            h->hashed_gen = h->state_gen;
+            h->hashed_step = h->step_index;
             uint64_t ub = h->n_ub;
             if (h->cfg.use_split) ub *= (h->cfg.split_ways == 4 ? 4u : 2u);
             h->n_ub = (uint32_t)std::min<uint64_t>(ub, h->cap);

@@ -217,24 +217,30 @@ __device__ __forceinline__ int row_range(const sph_config &c, const uint32_t *__
 }
 
 // ------------------------------------------------------------ 1. hash
+// Particle i at p: its cell key, and a slot among its cell's members from
+// the cell's counter (which must start the step at zero).  One atomic per
+// group of lanes in the same cell (consecutive particles often share one);
+// any distinct slots do, k_reorder restores the order.
+template <int DIM>
+__device__ __forceinline__ void hash_one(const sph_config &c, const WorkPtrs &w, uint32_t i, float4 p)
+{
+    const uint3 q = cell_of<DIM>(c, p);
+    const uint32_t k = key_of(c, q.x, q.y, q.z);
+    w.key[i] = k;
+    const unsigned grp = __match_any_sync(__activemask(), k);
+    const int lead = __ffs(grp) - 1, lane = threadIdx.x & 31;
+    uint32_t first = 0;
+    if (lane == lead) first = atomicAdd(w.cell_count + k, (uint32_t)__popc(grp));
+    first = __shfl_sync(grp, first, lead);
+    w.slot[i] = first + __popc(grp & ((1u << lane) - 1u));
+}
+
 template <int DIM>
 __device__ __forceinline__ void hash_body(const sph_config &c, const Counters *cnt, const CanonPtrs &st,
                                           const WorkPtrs &w)
 {
     const uint32_t n = cnt->n;
-    for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) {
-        uint3 q = cell_of<DIM>(c, st.pos[i]);
-        uint32_t k = key_of(c, q.x, q.y, q.z);
-        w.key[i] = k;
-        // one atomic per group of lanes in the same cell (consecutive particles
-        // often share one); any distinct slots do, k_reorder restores the order
-        const unsigned grp = __match_any_sync(__activemask(), k);
-        const int lead = __ffs(grp) - 1, lane = threadIdx.x & 31;
-        uint32_t first = 0;
-        if (lane == lead) first = atomicAdd(w.cell_count + k, (uint32_t)__popc(grp));
-        first = __shfl_sync(grp, first, lead);
-        w.slot[i] = first + __popc(grp & ((1u << lane) - 1u));
-    }
+    for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) hash_one<DIM>(c, w, i, st.pos[i]);
 }
 
 template <int DIM, int BS = kThreads>
@@ -1126,13 +1132,16 @@ __global__ void __launch_bounds__(BS) k_merge(sph_config c, const Counters *__re
 // 2D :1133-1160).  Writes the other canonical buffer.
 // ranks = false: the step ran no split and removal scans (split and merge
 // both off), so there are no children and nothing is removed.
+// hash_next: also hash every particle it writes for the next step (hash_one
+// at its new index; the cell counts were cleared after this step's scan), so
+// the next step starts at the cell scan.
 // Split groups: a parent and its children form a ring through `sibling`
 // (parent -> child 0 -> ... -> last child -> parent); a surviving member's
 // link follows the compaction; a merged survivor and everything else has none.
 template <int DIM>
 __device__ __forceinline__ void write_body(const sph_config &c, const Counters *cnt, Counters *cnt_next,
                                            const CanonPtrs &in, const CanonPtrs &out, const WorkPtrs &w,
-                                           bool ranks = true)
+                                           bool ranks = true, bool hash_next = false)
 {
     const uint32_t n = cnt->n;
     const uint32_t split_on = ranks && !cnt->split_off ? 1u : 0u;
@@ -1192,6 +1201,7 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
         const uint32_t sid = w.nscenes ? w.sscene[s] : 0u;   // a merge group never spans scenes
         if (w.nscenes) out.scene[dst] = sid;
         if (w.pos_comp) out.pos_lo[dst] = plo;
+        if (hash_next && !rm) hash_one<DIM>(c, w, dst, p);
         if (sp) {
             const uint32_t base = n - n_removed + w.split_rank[i] * extra;
             const float4 v0 = w.svel_n[s], e0 = w.sev_n[s], a0 = w.sacc_n[s];
@@ -1209,6 +1219,7 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
                 out.sibling[cd] = k + 1 < extra ? cd + 1 : dst;
                 if (w.nscenes) out.scene[cd] = sid;
                 if (w.pos_comp) out.pos_lo[cd] = plo_pre;
+                if (hash_next) hash_one<DIM>(c, w, cd, pc);
             }
         }
     }
@@ -1217,9 +1228,9 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
 template <int DIM, int BS = kThreads>
 __global__ void __launch_bounds__(BS) k_write(sph_config c, const Counters *__restrict__ cnt,
                                                    Counters *__restrict__ cnt_next, CanonPtrs in, CanonPtrs out,
-                                                   WorkPtrs w)
+                                                   WorkPtrs w, int hash_next)
 {
-    write_body<DIM>(c, cnt, cnt_next, in, out, w);
+    write_body<DIM>(c, cnt, cnt_next, in, out, w, true, hash_next != 0);
 }
 
 // ------------------------------------------------------------ reference-layout records

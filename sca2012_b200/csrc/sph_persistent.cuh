@@ -14,10 +14,11 @@
 //   [split scan (2 phases) + capacity guard | merge | removal scan (2 phases)] |
 //   write-out
 //
-// (the bracketed stages only when split or merge is on): 13 barriers per step
-// with adaptivity.  Without it the write-out runs in the energy stage and
-// hashes the next step's state too (write_hash_by_slot_body), so the next
-// step starts at the scan, and a small cell grid is scanned in one phase:
+// (the bracketed stages only when split or merge is on).  The write-out also
+// hashes the state it writes for the next step, so a step whose state was
+// written by a step before starts at the cell scan: 12 barriers per step with
+// adaptivity.  Without it the write-out runs in the energy stage
+// (write_hash_by_slot_body), and a small cell grid is scanned in one phase:
 // 5 barriers per step.  One launch runs several steps without splits, one
 // more barrier between two of them.  Each scan's second phase has every block sum
 // the block totals itself (scan_phase23_body) instead of one block scanning
@@ -76,8 +77,8 @@ struct PersistArgs {
 // slot s by the same thread (density, force and energy give slot s to the
 // same thread, and so does this loop).  So the thread that finished slot s's
 // energy writes the particle out right away, and hashes its new position for
-// the next step (the counts were cleared after this step's scan).  Values are
-// write_body's for a particle that neither splits nor merges.
+// the next step (hash_one; the counts were cleared after this step's scan).
+// Values are write_body's for a particle that neither splits nor merges.
 template <int DIM, int BS>
 __device__ __forceinline__ void write_hash_by_slot_body(const sph_config &c, const Counters *cnt, Counters *cnt_next,
                                                         const CanonPtrs &in, const CanonPtrs &out, const WorkPtrs &w)
@@ -94,34 +95,18 @@ __device__ __forceinline__ void write_hash_by_slot_body(const sph_config &c, con
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     for (uint32_t base = blockIdx.x * BS + wib * 32u; base < n; base += gridDim.x * BS) {
         const uint32_t s = base + lane;
-        const bool valid = s < n;
-        uint32_t k = 0;
-        uint32_t i = 0;
-        if (valid) {
-            i = w.sidx[s];
-            const float4 p = w.spos_n[s];
-            const float4 aux = w.saux[s];
-            out.pos[i] = p; out.vel[i] = w.svel_n[s]; out.ev[i] = w.sev_n[s]; out.acc[i] = w.sacc_n[s];
-            out.dens[i] = aux.x; out.press[i] = aux.y; out.energy[i] = w.senergy[s]; out.surface[i] = w.ssurf[s];
-            out.interior[i] = inter_rule ? w.sinter[s] : 0u;
-            const uint32_t j = in.sibling[i];
-            out.sibling[i] = j < n ? j : kEmpty;
-            if (w.nscenes) out.scene[i] = w.sscene[s];
-            if (w.pos_comp) out.pos_lo[i] = w.spos_lo_n[s];
-            const uint3 q = cell_of<DIM>(c, p);
-            k = key_of(c, q.x, q.y, q.z);
-        }
-        // the next step's hash of particle i (hash_body's slot assignment)
-        const unsigned vm = __ballot_sync(0xffffffffu, valid);
-        if (valid) {
-            w.key[i] = k;
-            const unsigned grp = __match_any_sync(vm, k);
-            const int lead = __ffs(grp) - 1;
-            uint32_t first = 0;
-            if (lane == lead) first = atomicAdd(w.cell_count + k, (uint32_t)__popc(grp));
-            first = __shfl_sync(grp, first, lead);
-            w.slot[i] = first + __popc(grp & ((1u << lane) - 1u));
-        }
+        if (s >= n) continue;
+        const uint32_t i = w.sidx[s];
+        const float4 p = w.spos_n[s];
+        const float4 aux = w.saux[s];
+        out.pos[i] = p; out.vel[i] = w.svel_n[s]; out.ev[i] = w.sev_n[s]; out.acc[i] = w.sacc_n[s];
+        out.dens[i] = aux.x; out.press[i] = aux.y; out.energy[i] = w.senergy[s]; out.surface[i] = w.ssurf[s];
+        out.interior[i] = inter_rule ? w.sinter[s] : 0u;
+        const uint32_t j = in.sibling[i];
+        out.sibling[i] = j < n ? j : kEmpty;
+        if (w.nscenes) out.scene[i] = w.sscene[s];
+        if (w.pos_comp) out.pos_lo[i] = w.spos_lo_n[s];
+        hash_one<DIM>(c, w, i, p);   // the next step's hash of particle i
     }
 }
 
@@ -247,7 +232,7 @@ __device__ __forceinline__ bool step_stages(const sph_config &c, Counters *cin, 
     if (!grid_scan<uint32_t>(a, k, cin, cout, w.removed_c, w.removed_rank, n, &cin->n_removed, 0, nullptr))
         return false;
     if (!grid_barrier(a, ++k, cin, cout)) return false;
-    write_body<DIM>(c, cin, cout, in, out, w, true);
+    write_body<DIM>(c, cin, cout, in, out, w, true, true);
     return true;
 }
 
@@ -280,7 +265,7 @@ __global__ void __launch_bounds__(BS, 2) k_step_persistent(sph_config c, Counter
         const int q = (p + j) & 1;
         Counters *cin = cnt + q, *cout = cnt + (q ^ 1);
         if (j > 0 && !grid_barrier(a, ++k, cin, cout)) return;
-        const bool hashed = j > 0 ? !a.ranks : a.hash_ready != 0;
+        const bool hashed = j > 0 || a.hash_ready != 0;
         if (!step_stages<DIM, BS>(c, cin, cout, buf.b[q], buf.b[q ^ 1], w, a, k, hashed, sm.pair, sm.merge))
             return;
     }
