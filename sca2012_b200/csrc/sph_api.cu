@@ -293,7 +293,7 @@ template <int DIM> int run_step(sph_handle *h, bool prologue = true)
     // density grid + surface mid-step: stale cell lists, integrated positions
     // (SPH-3D-2/sph_system.cpp:336-362)
     if (DIM == 3 && c.grid_every && h->mc.nodes && h->step_index % c.grid_every == 0) {
-        k_splat<<<grid_for(h, h->mc.nodes), kThreads, 0, s>>>(c, w.cell_off, w.spos_n, h->mc.dens);
+        k_splat<<<grid_for(h, h->mc.nodes / 2 + 1), kThreads, 0, s>>>(c, w.cell_off, w.spos_n, h->mc.dens);
         k_grid_normals<<<grid_for(h, h->mc.nodes), kThreads, 0, s>>>(c, h->mc.dens, h->mc.normal);
         h->last_launches += 2;
         run_mc(h);

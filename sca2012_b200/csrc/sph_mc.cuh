@@ -56,47 +56,84 @@ inline int mc_alloc(McBuffers &mc, const sph_config &c, std::vector<void *> &all
 // lower faces stay 0 (the reference's upper-face test never fires).  The
 // weight is m * poly6(R) * (R^2 - r^2)^3 with R the particle radius, or the
 // kernel length when splat_with_kernel is set.
+//
+// One thread per pair of x-adjacent nodes (2m-1, 2m): with two nodes per cell
+// edge both usually map to the same cell, so each candidate is loaded once
+// for two nodes.  Each node still sums exactly its own stencil's particles in
+// its own walk order (a node whose cell differs from its partner's takes the
+// candidates of the joint row range that fall in its own range).
 __global__ void __launch_bounds__(kThreads) k_splat(sph_config c, const uint32_t *__restrict__ off,
                                                    const float4 *__restrict__ pos, float *__restrict__ dens)
 {
     const uint32_t R = c.ndens[0], Cn = c.ndens[1], L = c.ndens[2];
-    const uint32_t G = R * Cn * L;
+    const uint32_t GX = R / 2 + 1;   // groups {0}, {1, 2}, {3, 4}, ...
+    const uint32_t G = GX * Cn * L;
+    // per level: the squared splat radius and m * W's coefficient
+    const float rad0 = c.splat_with_kernel ? c.kernel[0] : c.radius[0];
+    const float rad1 = c.splat_with_kernel ? c.kernel[1] : c.radius[1];
+    const float rs0 = __fmul_rn(rad0, rad0), rs1 = __fmul_rn(rad1, rad1);
+    const float cf0 = __fmul_rn(c.mass[0], c.splat_with_kernel ? c.poly6[0] : c.poly6_radius[0]);
+    const float cf1 = __fmul_rn(c.mass[1], c.splat_with_kernel ? c.poly6[1] : c.poly6_radius[1]);
     for (uint32_t g = grid_stride_start(); g < G; g += grid_stride()) {
-        const uint32_t vx = g % (R * Cn) % R, vy = g % (R * Cn) / R, vz = g / (R * Cn);
-        if (vx == 0 || vy == 0 || vz == 0) { dens[g] = 0.0f; continue; }
-        const float4 np = make_float4(__fmul_rn((float)vx, c.den_size), __fmul_rn((float)vy, c.den_size),
-                                      __fmul_rn((float)vz, c.den_size), 0.f);
+        const uint32_t gx = g % GX, vy = (g / GX) % Cn, vz = g / (GX * Cn);
+        const size_t row = ((size_t)vz * Cn + vy) * R;
+        const uint32_t va = 2u * gx - 1u, vb = 2u * gx;   // va is not a node when gx = 0
+        const bool has_b = vb < R;
+        if (gx == 0 || vy == 0 || vz == 0) {
+            if (gx > 0) dens[row + va] = 0.0f;
+            if (has_b) dens[row + vb] = 0.0f;
+            continue;
+        }
+        auto cell_x = [&](uint32_t vx) {
+            return min((uint32_t)floorf(__fmul_rn(__fdiv_rn((float)vx, (float)R), (float)c.ncell[0])),
+                       c.ncell[0] - 1);
+        };
         uint3 q;
-        q.x = (uint32_t)floorf(__fmul_rn(__fdiv_rn((float)vx, (float)R), (float)c.ncell[0]));
+        q.x = cell_x(va);
         q.y = (uint32_t)floorf(__fmul_rn(__fdiv_rn((float)vy, (float)Cn), (float)c.ncell[1]));
         q.z = (uint32_t)floorf(__fmul_rn(__fdiv_rn((float)vz, (float)L), (float)c.ncell[2]));
-        q.x = min(q.x, c.ncell[0] - 1); q.y = min(q.y, c.ncell[1] - 1); q.z = min(q.z, c.ncell[2] - 1);
-        float acc = 0.0f;
+        q.y = min(q.y, c.ncell[1] - 1); q.z = min(q.z, c.ncell[2] - 1);
+        const uint32_t qbx = has_b ? cell_x(vb) : q.x;
+        const float ny = __fmul_rn((float)vy, c.den_size), nz = __fmul_rn((float)vz, c.den_size);
+        const float4 npa = make_float4(__fmul_rn((float)va, c.den_size), ny, nz, 0.f);
+        const float4 npb = make_float4(__fmul_rn((float)vb, c.den_size), ny, nz, 0.f);
+        float acc_a = 0.0f, acc_b = 0.0f;
+        // acc += (m * W) * (rad^2 - r^2)^3 over r^2 < rad^2
+        auto add = [&](float &acc, const float4 &np, const float4 &pj, bool l1) {
+            float dx, dyy, dzz;
+            const float r2 = r2_of<3>(pj, np, dx, dyy, dzz);
+            const float rad2 = l1 ? rs0 : rs1;
+            const float x = __fsub_rn(rad2, r2);
+            if (r2 < rad2) acc = __fmaf_rn(l1 ? cf0 : cf1, __fmul_rn(__fmul_rn(x, x), x), acc);
+        };
+        const uint3 qb = make_uint3(qbx, q.y, q.z);
         for (int dz = -1; dz <= 1; ++dz)
             for (int dy = -1; dy <= 1; ++dy) {
-                uint32_t b, e;
-                if (!row_range<3>(c, off, q, dy, dz, b, e)) continue;
-                for (uint32_t t = b; t < e; ++t) {
-                    const float4 pj = pos[t];
-                    const int lj = lv(pj.w);
-                    const float rad = c.splat_with_kernel ? c.kernel[lj] : c.radius[lj];
-                    const float rad2 = __fmul_rn(rad, rad);
-                    float dx, dyy, dzz;
-                    const float r2 = r2_of<3>(pj, np, dx, dyy, dzz);
-                    if (r2 < rad2) {
-                        const float x = rad2 - r2;
-                        const float w = c.splat_with_kernel ? c.poly6[lj] : c.poly6_radius[lj];
-                        acc += c.mass[lj] * w * (x * x * x);
+                uint32_t ba, ea;
+                if (!row_range<3>(c, off, q, dy, dz, ba, ea)) continue;
+                if (qbx == q.x) {   // one stencil for both nodes
+                    for (uint32_t t = ba; t < ea; ++t) {
+                        const float4 pj = pos[t];
+                        const bool l1 = pj.w == 1.0f;
+                        add(acc_a, npa, pj, l1);
+                        add(acc_b, npb, pj, l1);
+                    }
+                } else {   // node b's row range starts and ends later in slot order
+                    uint32_t bb, eb;
+                    row_range<3>(c, off, qb, dy, dz, bb, eb);
+                    for (uint32_t t = ba; t < eb; ++t) {
+                        const float4 pj = pos[t];
+                        const bool l1 = pj.w == 1.0f;
+                        if (t < ea) add(acc_a, npa, pj, l1);
+                        if (t >= bb) add(acc_b, npb, pj, l1);
                     }
                 }
             }
-        dens[g] = acc;
+        dens[row + va] = acc_a;
+        if (has_b) dens[row + vb] = acc_b;
     }
 }
 
-// Grid normal = -grad(dens) by central differences, one-sided with 0 outside
-// the grid, divided by den_size and normalised (0 if zero)
-// (integrate_normall, SPH-3D-2/sph_system.cu:2221-2335).
 __global__ void __launch_bounds__(kThreads) k_grid_normals(sph_config c, const float *__restrict__ dens,
                                                           float4 *__restrict__ normal)
 {
