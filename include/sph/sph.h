@@ -240,14 +240,15 @@ int sph_set_scenes(sph_handle *h, uint32_t nscenes, const sph_scene *scenes);
  * launch overheads for small particle counts. */
 int sph_set_graph(sph_handle *h, int on);
 
-/* on != 0: sph_step runs each step as ONE cooperative launch (the stages
+/* on != 0: sph_step runs each step inside ONE cooperative launch (the stages
  * separated by grid-wide barriers instead of launch boundaries), for scenes
  * small enough that launches and the drain between them, not the work, set
- * the step time.  Results are bit for bit those of the ordinary launches;
- * steps that build the density grid and surface, and profiled steps, use
- * the ordinary launches.  Takes precedence over sph_set_graph.  No
- * counterpart in the reference, which launches every stage separately
- * (SPH-3D-2/sph_system.cpp:302-404).
+ * the step time.  Consecutive steps that cannot split (use_split = 0) share
+ * a launch, up to 256 of them, up to the next surface step.  Results are bit
+ * for bit those of the ordinary launches; steps that build the density grid
+ * and surface, and profiled steps, use the ordinary launches.  Takes
+ * precedence over sph_set_graph.  No counterpart in the reference, which
+ * launches every stage separately (SPH-3D-2/sph_system.cpp:302-404).
  * spin_limit: how many times a block polls a barrier before it gives up
  * (SPH_PERSISTENT_SPIN_DEFAULT: about a second; 0: at the first poll).  A
  * block that gives up ends the launch with SPH_ERR_TIMEOUT (reported by
@@ -326,7 +327,8 @@ int sph_write_pov_particles(const float *pos, const uint32_t *level, uint32_t n,
 /* Asynchronous readback: converts the current state to reference Particle
  * records on a side stream, writing them and the record count straight into
  * page-locked host memory that is mapped for the device (cudaHostAlloc with
- * cudaHostAllocMapped, or cudaHostRegister with cudaHostRegisterMapped).
+ * cudaHostAllocMapped, or cudaHostRegister with cudaHostRegisterMapped;
+ * both pointers 4-byte aligned, else SPH_ERR_INVALID).
  * Returns at once; the next sph_step overlaps the copy (it works on the other
  * state buffer) and a later step that would overwrite the buffer being read
  * waits for it.  sph_readback_wait blocks until the records and *count_dst
