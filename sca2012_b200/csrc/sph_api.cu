@@ -293,7 +293,9 @@ template <int DIM> int run_step(sph_handle *h, bool prologue = true)
     // density grid + surface mid-step: stale cell lists, integrated positions
     // (SPH-3D-2/sph_system.cpp:336-362)
     if (DIM == 3 && c.grid_every && h->mc.nodes && h->step_index % c.grid_every == 0) {
-        k_splat<<<grid_for(h, h->mc.nodes / 2 + 1), kThreads, 0, s>>>(c, w.cell_off, w.spos_n, h->mc.dens);
+        // one thread per node pair, uncapped: the block scheduler spreads the
+        // heavy pairs (cells of split particles hold four times the candidates)
+        k_splat<<<(h->mc.nodes / 2 + kThreads) / kThreads, kThreads, 0, s>>>(c, w.cell_off, w.spos_n, h->mc.dens);
         k_grid_normals<<<grid_for(h, h->mc.nodes), kThreads, 0, s>>>(c, h->mc.dens, h->mc.normal);
         h->last_launches += 2;
         run_mc(h);
