@@ -428,7 +428,7 @@ int sph_conserved(sph_handle *h, double out[7]);
  * the candidates on the handle's current state (the state is restored after
  * every trial and at the end), `reps` steps per candidate, stage by stage, and
  * keeps the fastest; block in {128, 256, 512} (force and energy: 128, 256;
- * force with and without a register cap), blocks_per_sm in {2, 4, 8, 16, 32}.
+ * force with and without a register cap), blocks_per_sm in {2, 4, 8, 16, 32, 64}.
  * Defaults: 256 threads, 8 per SM, no cap.
  */
 #define SPH_TUNE_HASH     0

@@ -1428,7 +1428,7 @@ int sph_autotune(sph_handle *h, uint32_t reps, sph_tuning *out)
     int rc = trial();
     const float before = step_ms / reps;
     static const uint32_t kBs[3] = {128, 256, 512};
-    static const uint32_t kBpsm[5] = {2, 4, 8, 16, 32};
+    static const uint32_t kBpsm[6] = {2, 4, 8, 16, 32, 64};
     for (int st = 0; st < SPH_TUNE_STAGES && !rc; ++st) {
         if (st == SPH_TUNE_MERGE && !h->cfg.use_merge) continue;
         const uint32_t inc_bs = h->tune_bs[st], inc_bp = h->tune_bpsm[st], inc_cap = h->tune_minb[st];
