@@ -255,8 +255,13 @@ template <bool NC>
 __device__ __forceinline__ void scatter_body(const Counters *cnt, const WorkPtrs &w)
 {
     const uint32_t n = cnt->n;
-    for (uint32_t i = grid_stride_start(); i < n; i += grid_stride())
-        w.tmp[ldro<NC>(w.cell_off + w.key[i]) + w.slot[i]] = i;
+    for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) {
+        // always below n when the counts, keys and slots come from one hash;
+        // the test keeps a state left inconsistent by an abandoned persistent
+        // step (SPH_ERR_TIMEOUT, not yet replaced by sph_set_state) in bounds
+        const uint32_t d = ldro<NC>(w.cell_off + w.key[i]) + w.slot[i];
+        if (d < n) w.tmp[d] = i;
+    }
 }
 
 template <int BS = kThreads>
