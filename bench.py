@@ -622,6 +622,8 @@ def batched_scenes(args, rank=0, world=1):
         bs.append(h)
         particles += len(pos)
     timed(bs, 3)
+    # launch shapes picked by the autotuner on each handle's state (restored afterwards)
+    tuned = [None if args.no_autotune else h.autotune(reps=2) for h in bs]
     t_batched = timed(bs, steps)
     # the same steps with plain launches: what graph replay saves, i.e. the
     # launch overhead a single persistent launch per step could remove at most
@@ -698,6 +700,8 @@ def batched_scenes(args, rank=0, world=1):
             "batched_eager_launches_ms_per_step": t_eager / steps * 1e3,
             "batched_persistent_ms_per_step": t_persist / steps * 1e3,
             "batched_persistent_scene_steps_per_s": n_sc * steps / t_persist, "status": status,
+            "tuning": [None if t is None else {"block": t["block"], "blocks_per_sm": t["blocks_per_sm"]}
+                       for t in tuned],
             "adjoint_last_50": {"forward_ms_per_step": t_fwd / adj_steps * 1e3,
                                 "backward_ms_per_step": t_bwd / adj_steps * 1e3,
                                 "backward_vs_forward": t_bwd / t_fwd,
