@@ -429,7 +429,8 @@ int sph_conserved(sph_handle *h, double out[7]);
  * every trial and at the end), `reps` steps per candidate, stage by stage, and
  * keeps the fastest; block in {128, 256, 512} (force and energy: 128, 256;
  * force with and without a register cap), blocks_per_sm in {2, 4, 8, 16, 32, 64}.
- * Defaults: 256 threads, 8 per SM, no cap.
+ * Defaults: 256 threads and 8 per SM for hash, scatter, reorder and merge;
+ * 128 threads and 64 per SM for density, force, energy and write; no cap.
  */
 #define SPH_TUNE_HASH     0
 #define SPH_TUNE_SCATTER  1

@@ -78,8 +78,12 @@ struct sph_handle {
     uint64_t state_gen = 0;
     // launch shape per tuned stage (sph_set_tuning / sph_autotune)
     double *cons = nullptr;   // conserved-quantity partial sums (allocated on first use)
-    uint32_t tune_bs[SPH_TUNE_STAGES] = {256, 256, 256, 256, 256, 256, 256, 256};
-    uint32_t tune_bpsm[SPH_TUNE_STAGES] = {8, 8, 8, 8, 8, 8, 8, 8};
+    // defaults: the streaming stages at full occupancy with grid-stride loops;
+    // density, force, energy and write one particle per thread in 128-thread
+    // blocks (many more blocks than fit at once, so the block scheduler evens
+    // out warps of unequal work), the autotuner's usual choice on 1M particles
+    uint32_t tune_bs[SPH_TUNE_STAGES] = {256, 256, 256, 128, 128, 128, 256, 128};
+    uint32_t tune_bpsm[SPH_TUNE_STAGES] = {8, 8, 8, 64, 64, 64, 8, 64};
     uint32_t tune_minb[SPH_TUNE_STAGES] = {0, 0, 0, 0, 0, 1, 0, 0};   // 1: register-capped variant
     // persistent step: the whole step as one cooperative launch
     bool persistent = false;
