@@ -423,11 +423,9 @@ def run_ours(args, rank, world, local_rank):
                 n_sum += n_here
                 d2h_f += n_here * rec
             else:
-                rc = s._lib.sph_read_particles_async(s._h, fbufs[k & 1].data_ptr(), cap_bytes,
-                                                     fcnts[k & 1].data_ptr())
-                assert rc == 0, s._lib.sph_last_error(s._h)
+                s.read_particles_async_into(fbufs[k & 1].data_ptr(), cap_bytes, fcnts[k & 1].data_ptr())
         if mode == "async":
-            assert s._lib.sph_readback_wait(s._h) == 0
+            s.readback_wait()
         b.record(stream)
         b.synchronize()
         if mode == "async":   # the count moves by well under 1 % over these steps

@@ -219,6 +219,17 @@ class Solver:
     def write_particles_from(self, host_ptr, n):
         self._check(self._lib.sph_write_particles(self._h, C.c_void_p(host_ptr), int(n)), "sph_write_particles")
 
+    def read_particles_async_into(self, mapped_ptr, capacity_bytes, mapped_count_ptr):
+        """Starts the asynchronous readback of the current state as reference
+        Particle records into mapped page-locked memory (4-byte aligned), the
+        record count into *mapped_count_ptr; returns at once (sph_read_particles_async)."""
+        self._check(self._lib.sph_read_particles_async(self._h, C.c_void_p(mapped_ptr), int(capacity_bytes),
+                                                       C.c_void_p(mapped_count_ptr)), "sph_read_particles_async")
+
+    def readback_wait(self):
+        """Blocks until every asynchronous readback has landed in host memory."""
+        self._check(self._lib.sph_readback_wait(self._h), "sph_readback_wait")
+
     def read_particles(self):
         """Reference-layout records as a numpy structured array."""
         n = self.num_particles()

@@ -201,8 +201,8 @@ def test_persistent_multi_step_launch_waits_for_readbacks(gpu):
     cnts = [torch.zeros(1, dtype=torch.int32, pin_memory=True) for _ in range(2)]
     for j, k in enumerate((1, 3)):
         s.step(k)
-        assert s._lib.sph_read_particles_async(s._h, bufs[j].data_ptr(), nbytes, cnts[j].data_ptr()) == 0
-    assert s._lib.sph_readback_wait(s._h) == 0
+        s.read_particles_async_into(bufs[j].data_ptr(), nbytes, cnts[j].data_ptr())
+    s.readback_wait()
     assert s.sync_status() == 0
     assert s.last_launch_count() == 1
     s.close()
