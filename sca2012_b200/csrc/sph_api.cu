@@ -84,7 +84,7 @@ struct sph_handle {
     // out warps of unequal work), the autotuner's usual choice on 1M particles
     uint32_t tune_bs[SPH_TUNE_STAGES] = {256, 256, 256, 128, 128, 128, 256, 128};
     uint32_t tune_bpsm[SPH_TUNE_STAGES] = {8, 8, 8, 64, 64, 64, 8, 64};
-    uint32_t tune_minb[SPH_TUNE_STAGES] = {0, 0, 0, 0, 0, 1, 0, 0};   // 1: register-capped variant
+    uint32_t tune_minb[SPH_TUNE_STAGES] = {0, 0, 0, 0, 0, 0, 0, 0};   // 1: register-capped variant
     // persistent step: the whole step as one cooperative launch
     bool persistent = false;
     uint32_t spin_limit = SPH_PERSISTENT_SPIN_DEFAULT;
