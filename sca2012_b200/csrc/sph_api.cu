@@ -214,7 +214,8 @@ void scan_u32(sph_handle *h, const uint32_t *in, uint32_t *out, const uint32_t *
 void run_mc(sph_handle *h)
 {
     McBuffers &mc = h->mc;
-    const uint32_t GQ = grid_for(h, mc.cubes);
+    // one thread per cube: every thread's corner loads are in flight at once
+    const uint32_t GQ = (mc.cubes + kThreads - 1) / kThreads;
     k_mc_count<<<GQ, kThreads, 0, h->stream>>>(h->cfg, mc.dens, mc.cube_cnt);
     scan_u32(h, mc.cube_cnt, mc.cube_off, nullptr, mc.cubes, mc.num_tri, 0, nullptr);
     k_mc_emit<<<GQ, kThreads, 0, h->stream>>>(h->cfg, mc.dens, mc.normal, mc.cube_cnt, mc.cube_off, mc.max_tri,
@@ -300,7 +301,7 @@ template <int DIM> int run_step(sph_handle *h, bool prologue = true)
         // one thread per node pair, uncapped: the block scheduler spreads the
         // heavy pairs (cells of split particles hold four times the candidates)
         k_splat<<<(h->mc.nodes / 2 + kThreads) / kThreads, kThreads, 0, s>>>(c, w.cell_off, w.spos_n, h->mc.dens);
-        k_grid_normals<<<grid_for(h, h->mc.nodes), kThreads, 0, s>>>(c, h->mc.dens, h->mc.normal);
+        k_grid_normals<<<(h->mc.nodes + kThreads - 1) / kThreads, kThreads, 0, s>>>(c, h->mc.dens, h->mc.normal);
         h->last_launches += 2;
         run_mc(h);
         h->grid_valid = true;
