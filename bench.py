@@ -308,6 +308,7 @@ def run_ours(args, rank, world, local_rank):
         launches += s.last_launch_count()
     torch.cuda.synchronize()
     clk = clocks.stop()
+    last_step = s.last_step_stats()   # synchronises; after the timed steps
     s.set_graph(False)
     status = s.sync_status()
     cons1 = s.conserved()
@@ -485,6 +486,7 @@ def run_ours(args, rank, world, local_rank):
                        "launch": "CUDA graph replay per step (surface steps launch directly)",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "plain_value": plain_value, "adaptive_vs_plain": value / plain_value,
+            "last_timed_step": last_step,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // e2e_steps,
                     "d2h_bytes_per_step": d2h // e2e_steps,
                     "api": "sph_write_particles + sph_step + sph_read_particles (page-locked host)",

@@ -300,6 +300,18 @@ int sph_set_debug(sph_handle *h, int on);
 /* Number of kernel launches the last sph_step issued. */
 int sph_last_launch_count(const sph_handle *h, uint32_t *launches);
 
+/* Particle counts of the last step (the per-step line the reference's
+ * SPH-3D-4 app prints as its L/S counts, SPH-3D-4/sph_main.cpp:819, and the
+ * split/merge activity behind it).  Synchronises with the handle's stream.
+ * n_split: particles that split (0 when the capacity guard suppressed the
+ * step's splits, split_suppressed = 1); n_removed: particles merged away;
+ * n_end = n_start + n_split * (ways - 1) - n_removed; n_level2: level-2
+ * particles after the step; error: the step's SPH_ERR_* bits (1 << code). */
+typedef struct {
+    uint32_t n_start, n_split, n_removed, n_end, n_level2, split_suppressed, error;
+} sph_step_stats;
+int sph_last_step_stats(sph_handle *h, sph_step_stats *out);
+
 /* Density grid of the current state (splat + normals on the device), copied
  * to host arrays of ndens[0]*ndens[1]*ndens[2] floats / 3*that floats. */
 int sph_density_grid(sph_handle *h, float *dens, float *normal);

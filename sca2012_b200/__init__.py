@@ -352,6 +352,13 @@ class Solver:
         """Synchronises and returns the device status code (0 = ok) without raising."""
         return int(self._lib.sph_sync(self._h))
 
+    def last_step_stats(self):
+        """Counts of the last step: n_start, n_split, n_removed, n_end,
+        n_level2, split_suppressed, error (sph_last_step_stats)."""
+        st = _abi.StepStats()
+        self._check(self._lib.sph_last_step_stats(self._h, C.byref(st)), "sph_last_step_stats")
+        return {k: int(getattr(st, k)) for k, _ in st._fields_}
+
     def last_launch_count(self):
         n = C.c_uint32()
         self._check(self._lib.sph_last_launch_count(self._h, C.byref(n)), "sph_last_launch_count")

@@ -126,6 +126,11 @@ class Tuning(C.Structure):
                 ("reg_cap", C.c_uint32 * TUNE_STAGES), ("step_ms_before", C.c_float), ("step_ms_after", C.c_float)]
 
 
+class StepStats(C.Structure):
+    _fields_ = [(k, C.c_uint32) for k in ("n_start", "n_split", "n_removed", "n_end", "n_level2",
+                                           "split_suppressed", "error")]
+
+
 H = C.c_void_p
 DP = C.POINTER(C.c_double)
 
@@ -156,6 +161,7 @@ SIGNATURES = [
     ("sph_set_stream", C.c_int, [H, C.c_void_p]),
     ("sph_set_debug", C.c_int, [H, C.c_int]),
     ("sph_last_launch_count", C.c_int, [H, UP]),
+    ("sph_last_step_stats", C.c_int, [H, C.c_void_p]),
     ("sph_density_grid", C.c_int, [H, FP, FP]),
     ("sph_extract_surface", C.c_int, [H, C.POINTER(MeshView)]),
     ("sph_surface_from_grid", C.c_int, [H, FP, FP, C.POINTER(MeshView)]),

@@ -39,6 +39,7 @@ struct sph_handle {
     WorkPtrs w;
     uint32_t *scan_blocks = nullptr;  // kScanBlocks * 2 u32
     uint32_t *scan_grand = nullptr;   // scratch total
+    uint32_t *stat_buf = nullptr;     // sph_last_step_stats: level-2 count
     uint32_t n_ub = 0;                // host upper bound of the live count
     uint32_t n_last_sorted = 0;       // count the last step started with (host copy)
     bool have_step = false;
@@ -607,6 +608,7 @@ int sph_create(const sph_config *cfg, sph_handle **out)
     rc |= dalloc(h, &w.macc, cap); rc |= dalloc(h, &w.menergy, cap);
     rc |= dalloc(h, &h->scan_blocks, (size_t)kScanBlocks * 2);
     rc |= dalloc(h, &h->scan_grand, 4);
+    rc |= dalloc(h, &h->stat_buf, 4);
     rc |= dalloc(h, &h->gsync, 2);
     if (!rc) rc = mc_alloc(h->mc, *cfg, h->allocs);
     if (rc) {
@@ -1224,6 +1226,30 @@ int sph_last_launch_count(const sph_handle *h, uint32_t *launches)
     if (!h || !launches) return SPH_ERR_INVALID;
     *launches = h->last_launches;
     return SPH_OK;
+}
+
+int sph_last_step_stats(sph_handle *h, sph_step_stats *out)
+{
+    if (!h || !out) return SPH_ERR_INVALID;
+    if (!h->have_step) { h->err = "no step run since the last state change"; return SPH_ERR_INVALID; }
+    cudaStream_t s = h->stream;
+    cudaMemsetAsync(h->stat_buf, 0, sizeof(uint32_t), s);
+    k_count_level2<<<grid_for(h, h->n_ub), kThreads, 0, s>>>(h->cnt + h->cur, h->buf[h->cur].pos, h->stat_buf);
+    Counters c[2];
+    uint32_t level2 = 0;
+    cudaMemcpyAsync(c, h->cnt, sizeof(c), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&level2, h->stat_buf, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { h->err = cudaGetErrorString(e); return SPH_ERR_CUDA; }
+    const Counters &last = c[h->cur ^ 1], &now = c[h->cur];   // the last step's input, its output
+    out->n_start = last.n;
+    out->split_suppressed = last.split_off ? 1u : 0u;
+    out->n_split = last.split_off ? 0u : last.n_split;
+    out->n_removed = last.n_removed;
+    out->n_end = now.n;
+    out->n_level2 = level2;
+    out->error = now.error;
+    return cuda_check(h, "sph_last_step_stats");
 }
 
 int sph_set_debug(sph_handle *h, int on)

@@ -1370,6 +1370,17 @@ __global__ void __launch_bounds__(kThreads) k_conserved(sph_config c, const Coun
     }
 }
 
+// Level-2 particles of the state (sph_last_step_stats): *out += the count.
+__global__ void __launch_bounds__(kThreads) k_count_level2(const Counters *__restrict__ cnt,
+                                                          const float4 *__restrict__ pos, uint32_t *out)
+{
+    const uint32_t n = cnt->n;
+    uint32_t k = 0;
+    for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) k += pos[i].w != 1.0f ? 1u : 0u;
+    k = __reduce_add_sync(0xffffffffu, k);
+    if ((threadIdx.x & 31) == 0 && k) atomicAdd(out, k);
+}
+
 __global__ void k_conserved_final(const double *partial, uint32_t blocks, double *out)
 {
     if (threadIdx.x < kConservedTerms) {
