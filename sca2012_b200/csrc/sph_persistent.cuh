@@ -2,8 +2,8 @@
 //
 // The reference launches every stage of a step separately
 // (SPHSystem::animation, SPH-3D-2/sph_system.cpp:302-404; animate,
-// SPH-2D/sph_system.cpp:190-264), and so does sph_step's ordinary path (about
-// 19 launches, or one replayed CUDA graph of them).  On small scenes the step
+// SPH-2D/sph_system.cpp:190-264), and so does sph_step's ordinary path (13
+// launches and a memset, or one replayed CUDA graph of them).  On small scenes the step
 // is then bound by the launches and the drain between them, not by the work.
 // k_step_persistent runs the same stage bodies (sph_kernels.cuh,
 // sph_scan.cuh) in one launch whose blocks are all resident (a cooperative
@@ -39,6 +39,9 @@
 // kernel always ends.  The input state buffer is never written, but the step
 // that gave up writes no output: the state after a timeout must be restored
 // (sph_set_state).  A step whose input carries the timeout bit does nothing.
+// A launch of several steps alternates the two state buffers and counters
+// as that many separate steps would (the grid is sized for the first step's
+// count, so only steps that cannot split share a launch).
 // No stage reads data through the non-coherent path (loads are NC = false),
 // since a stage reads what an earlier stage of the same launch wrote.
 #pragma once
