@@ -201,13 +201,16 @@ uint64_t launch_key(const sph_handle *h)
     default: { constexpr int B = 256, M = 3; __VA_ARGS__; } break;                      \
     }
 
-// Exclusive scan of u32 `in` -> `out`; length from len_ptr (device) or len_const.
+// Exclusive scan of u32 `in` -> `out`; length from len_ptr (device) or
+// len_const.  skip_if_zero: a device count of the nonzero inputs (0: the
+// output is all zeros and is written without a scan).
 void scan_u32(sph_handle *h, const uint32_t *in, uint32_t *out, const uint32_t *len_ptr, uint32_t len_const,
-              uint32_t *grand, int total_at_len, uint32_t *list)
+              uint32_t *grand, int total_at_len, uint32_t *list, const uint32_t *skip_if_zero = nullptr)
 {
-    scan_phase1<uint32_t><<<kScanBlocks, kScanThreads, 0, h->stream>>>(in, len_ptr, len_const, h->scan_blocks);
+    scan_phase1<uint32_t><<<kScanBlocks, kScanThreads, 0, h->stream>>>(in, len_ptr, len_const, h->scan_blocks,
+                                                                       skip_if_zero);
     scan_phase23<uint32_t><<<kScanBlocks, kScanThreads, 0, h->stream>>>(in, out, len_ptr, len_const, h->scan_blocks,
-                                                                        grand, total_at_len, list);
+                                                                        grand, total_at_len, list, skip_if_zero);
     h->last_launches += 2;
 }
 
@@ -313,7 +316,7 @@ template <int DIM> int run_step(sph_handle *h, bool prologue = true)
                                                                                           h->debug ? 1 : 0));
     stage(h, "energy_split");
     h->last_launches += 6;
-    scan_u32(h, w.split_c, w.split_rank, &cin->n, 0, &cin->n_split, 0, w.split_list);
+    scan_u32(h, w.split_c, w.split_rank, &cin->n, 0, &cin->n_split, 0, w.split_list, &cin->split_flags);
     k_split_guard<<<1, 1, 0, s>>>(c, cin, h->cap);
     h->last_launches += 1;
     stage(h, "scan_split");
@@ -324,7 +327,7 @@ template <int DIM> int run_step(sph_handle *h, bool prologue = true)
         h->last_launches += 1;
         stage(h, "merge");
     }
-    scan_u32(h, w.removed_c, w.removed_rank, &cin->n, 0, &cin->n_removed, 0, nullptr);
+    scan_u32(h, w.removed_c, w.removed_rank, &cin->n, 0, &cin->n_removed, 0, nullptr, &cin->removed_flags);
     stage(h, "scan_removed");
     SPH_BS_SWITCH(h->tune_bs[SPH_TUNE_WRITE],
                   k_write<DIM, B><<<grid_st(h, nub, SPH_TUNE_WRITE), B, 0, s>>>(c, cin, cout, in, out, w, 1));

@@ -44,7 +44,9 @@ struct Counters {
     uint32_t error;        // SPH_ERR_* bit flags (1 << code)
     uint32_t split_off;    // 1: splits suppressed this step (capacity)
     uint32_t disp2_max;    // bits of the step's largest squared displacement (FP32 >= 0), by the force pass
-    uint32_t pad[2];
+    uint32_t split_flags;  // particles the energy pass flagged to split this step
+    uint32_t removed_flags;  // particles the merge pass flagged as merged away this step
+                           // (a rank scan whose flags are all zero writes zeros instead of scanning)
 };
 
 struct CanonPtrs {
@@ -865,6 +867,7 @@ __device__ __forceinline__ void energy_split_body(const sph_config &c, Counters 
                 split = split_score(c, energy, surf) > c.split_criteria ? 1u : 0u;
         }
         w.split_c[i] = split;
+        if (split) atomicAdd(&cnt->split_flags, 1u);
         w.removed_c[i] = 0u;
         if (c.merge_rule == SPH_MERGE_INTERIOR || c.merge_rule == SPH_MERGE_SIBLING) {
             const int flagged = nb < c.split_min_neighbors || dens < c.split_density_ratio * c.rest_density;
@@ -926,7 +929,7 @@ __device__ __forceinline__ int merge_eligible(const sph_config &c, const WorkPtr
 // Merges the group g[0..ways) into g[0] (values on the post-split state).
 template <int DIM>
 __device__ __forceinline__ void merge_group(const sph_config &c, const WorkPtrs &w, const uint32_t *g,
-                                            uint32_t ways, uint32_t split_on, float hs2)
+                                            uint32_t ways, uint32_t split_on, float hs2, uint32_t *removed_flags)
 {
     float V[4], Vs = 0.f;
     for (uint32_t k = 0; k < ways; ++k) {
@@ -959,6 +962,7 @@ __device__ __forceinline__ void merge_group(const sph_config &c, const WorkPtrs 
     w.menergy[t1] = en / (float)ways;
     w.leader[t1] = 1u;
     for (uint32_t k = 1; k < ways; ++k) w.removed_c[w.sidx[g[k]]] = 1u;
+    atomicAdd(removed_flags, ways - 1u);
     if (w.merge_to) {   // recorded for the adjoint
         for (uint32_t k = 0; k < ways; ++k) w.merge_to[g[k]] = t1;
         w.mvs[t1] = Vs;
@@ -973,7 +977,7 @@ struct MergeSmem {
 };
 
 template <int DIM>
-__device__ __forceinline__ void merge_body(const sph_config &c, const Counters *cnt, const CanonPtrs &st,
+__device__ __forceinline__ void merge_body(const sph_config &c, Counters *cnt, const CanonPtrs &st,
                                            const WorkPtrs &w, uint32_t ncells, uint32_t cap, MergeSmem *ms)
 {
     const unsigned full = 0xffffffffu;
@@ -1041,7 +1045,7 @@ __device__ __forceinline__ void merge_body(const sph_config &c, const Counters *
             for (uint32_t k = lane; k < len; k += 32)
                 if (ms[wib].lrank[k] % ways == 0 && k + ways - 1 < len &&
                     ms[wib].lcell[k + ways - 1] == ms[wib].lcell[k])
-                    merge_group<DIM>(c, w, &ms[wib].list[k], ways, split_on, hs2);
+                    merge_group<DIM>(c, w, &ms[wib].list[k], ways, split_on, hs2, &cnt->removed_flags);
             __syncwarp();
             continue;
         }
@@ -1067,7 +1071,7 @@ __device__ __forceinline__ void merge_body(const sph_config &c, const Counters *
             const uint32_t groups = count / ways;
             if (count <= (uint32_t)kMergeListMax) {
                 for (uint32_t g = lane; g < groups; g += 32)
-                    merge_group<DIM>(c, w, &ms[wib].list[g * ways], ways, split_on, hs2);
+                    merge_group<DIM>(c, w, &ms[wib].list[g * ways], ways, split_on, hs2, &cnt->removed_flags);
             } else if (lane == 0) {
                 // more eligible members than the list holds: walk the cell
                 // serially with the same group arithmetic
@@ -1076,7 +1080,7 @@ __device__ __forceinline__ void merge_body(const sph_config &c, const Counters *
                     if (!merge_eligible<DIM>(c, w, t, split_on, ways, cell_score)) continue;
                     grp[got++] = t;
                     if (got == ways) {
-                        merge_group<DIM>(c, w, grp, ways, split_on, hs2);
+                        merge_group<DIM>(c, w, grp, ways, split_on, hs2, &cnt->removed_flags);
                         got = 0;
                         ++done;
                     }
@@ -1094,7 +1098,7 @@ __device__ __forceinline__ void merge_body(const sph_config &c, const Counters *
 // is averaged in ring order from it, with merge_group's weights.  One thread
 // per particle; only the survivor-to-be writes, so no group is merged twice.
 template <int DIM>
-__device__ __forceinline__ void merge_sibling_body(const sph_config &c, const Counters *cnt, const CanonPtrs &st,
+__device__ __forceinline__ void merge_sibling_body(const sph_config &c, Counters *cnt, const CanonPtrs &st,
                                                    const WorkPtrs &w)
 {
     const uint32_t n = cnt->n;
@@ -1117,12 +1121,12 @@ __device__ __forceinline__ void merge_sibling_body(const sph_config &c, const Co
                 j = st.sibling[j];
             }
         }
-        if (ok && j == i) merge_group<DIM>(c, w, g, ways, split_on, hs2);
+        if (ok && j == i) merge_group<DIM>(c, w, g, ways, split_on, hs2, &cnt->removed_flags);
     }
 }
 
 template <int DIM, int BS = kThreads>
-__global__ void __launch_bounds__(BS) k_merge(sph_config c, const Counters *__restrict__ cnt,
+__global__ void __launch_bounds__(BS) k_merge(sph_config c, Counters *__restrict__ cnt,
                                                    CanonPtrs st, WorkPtrs w, uint32_t ncells, uint32_t cap)
 {
     __shared__ MergeSmem ms[BS / 32];
@@ -1163,6 +1167,8 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
         cnt_next->n_split = 0;
         cnt_next->n_removed = 0;
         cnt_next->split_off = 0;
+        cnt_next->split_flags = 0;
+        cnt_next->removed_flags = 0;
     }
     // one thread per particle index: reads gather from the sorted slot, the
     // writes (survivors keep their order) stay coalesced

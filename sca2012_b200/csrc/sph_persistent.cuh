@@ -93,6 +93,8 @@ __device__ __forceinline__ void write_hash_by_slot_body(const sph_config &c, con
         cnt_next->n_split = 0;
         cnt_next->n_removed = 0;
         cnt_next->split_off = 0;
+        cnt_next->split_flags = 0;
+        cnt_next->removed_flags = 0;
     }
     const bool inter_rule = c.merge_rule == SPH_MERGE_INTERIOR || c.merge_rule == SPH_MERGE_SIBLING;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -223,8 +225,14 @@ __device__ __forceinline__ bool step_stages(const sph_config &c, Counters *cin, 
     }
     if (!grid_barrier(a, ++k, cin, cout)) return false;
     const uint32_t n = cin->n;
-    if (!grid_scan<uint32_t>(a, k, cin, cout, w.split_c, w.split_rank, n, &cin->n_split, 0, w.split_list))
-        return false;
+    // a scan of all-zero flags is all zeros: written directly, no barrier
+    if (cin->split_flags) {
+        if (!grid_scan<uint32_t>(a, k, cin, cout, w.split_c, w.split_rank, n, &cin->n_split, 0, w.split_list))
+            return false;
+    } else {
+        for (uint32_t q = grid_stride_start(); q < n; q += grid_stride()) w.split_rank[q] = 0u;
+        if (blockIdx.x == 0 && threadIdx.x == 0) cin->n_split = 0u;
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) split_guard_body(c, cin, a.cap);
     if (!grid_barrier(a, ++k, cin, cout)) return false;
     if (c.use_merge) {
@@ -232,8 +240,13 @@ __device__ __forceinline__ bool step_stages(const sph_config &c, Counters *cin, 
         else merge_body<DIM>(c, cin, in, w, a.ncells, a.cap, merge);
         if (!grid_barrier(a, ++k, cin, cout)) return false;
     }
-    if (!grid_scan<uint32_t>(a, k, cin, cout, w.removed_c, w.removed_rank, n, &cin->n_removed, 0, nullptr))
-        return false;
+    if (cin->removed_flags) {
+        if (!grid_scan<uint32_t>(a, k, cin, cout, w.removed_c, w.removed_rank, n, &cin->n_removed, 0, nullptr))
+            return false;
+    } else {
+        for (uint32_t q = grid_stride_start(); q < n; q += grid_stride()) w.removed_rank[q] = 0u;
+        if (blockIdx.x == 0 && threadIdx.x == 0) cin->n_removed = 0u;
+    }
     if (!grid_barrier(a, ++k, cin, cout)) return false;
     write_body<DIM>(c, cin, cout, in, out, w, true, true);
     return true;

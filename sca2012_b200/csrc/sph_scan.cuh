@@ -88,10 +88,14 @@ __device__ __forceinline__ void scan_phase1_body(const T *in, uint32_t len, T *b
     if (threadIdx.x == 0) block_tot[blockIdx.x] = tot;
 }
 
+// skip_if_zero (optional): a count of the nonzero inputs; at 0 the scan is
+// all zeros, which scan_phase23 writes without reading the input.
 template <typename T>
 __global__ void __launch_bounds__(kScanThreads) scan_phase1(const T *__restrict__ in, const uint32_t *len_ptr,
-                                                           uint32_t len_const, T *__restrict__ block_tot)
+                                                           uint32_t len_const, T *__restrict__ block_tot,
+                                                           const uint32_t *skip_if_zero = nullptr)
 {
+    if (skip_if_zero && *skip_if_zero == 0u) return;
     scan_phase1_body<T>(in, len_ptr ? *len_ptr : len_const, block_tot);
 }
 
@@ -242,9 +246,20 @@ template <typename T>
 __global__ void __launch_bounds__(kScanThreads) scan_phase23(const T *__restrict__ in, T *__restrict__ out,
                                                             const uint32_t *len_ptr, uint32_t len_const,
                                                             const T *__restrict__ block_tot, T *grand,
-                                                            int out_total_at_len, uint32_t *list)
+                                                            int out_total_at_len, uint32_t *list,
+                                                            const uint32_t *skip_if_zero = nullptr)
 {
-    scan_phase23_body<T>(in, out, len_ptr ? *len_ptr : len_const, block_tot, grand, out_total_at_len, list);
+    const uint32_t len = len_ptr ? *len_ptr : len_const;
+    if (skip_if_zero && *skip_if_zero == 0u) {   // every input is zero: so is every output
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x)
+            out[i] = zero_of<T>();
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            if (grand) *grand = zero_of<T>();
+            if (out_total_at_len) out[len] = zero_of<T>();
+        }
+        return;
+    }
+    scan_phase23_body<T>(in, out, len, block_tot, grand, out_total_at_len, list);
 }
 
 template <typename T>
