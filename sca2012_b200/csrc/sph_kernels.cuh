@@ -47,6 +47,8 @@ struct Counters {
     uint32_t split_flags;  // particles the energy pass flagged to split this step
     uint32_t removed_flags;  // particles the merge pass flagged as merged away this step
                            // (a rank scan whose flags are all zero writes zeros instead of scanning)
+    uint32_t merge_candidates;  // particles that may be merge-eligible this step, by the energy
+                           // pass (at 0 the merge pass has nothing to do and returns at once)
 };
 
 struct CanonPtrs {
@@ -869,9 +871,23 @@ __device__ __forceinline__ void energy_split_body(const sph_config &c, Counters 
         w.split_c[i] = split;
         if (split) atomicAdd(&cnt->split_flags, 1u);
         w.removed_c[i] = 0u;
+        uint32_t inter = 0;
         if (c.merge_rule == SPH_MERGE_INTERIOR || c.merge_rule == SPH_MERGE_SIBLING) {
             const int flagged = nb < c.split_min_neighbors || dens < c.split_density_ratio * c.rest_density;
-            w.sinter[s] = (flagged || split) ? 0u : st.interior[i] + 1u;
+            inter = (flagged || split) ? 0u : st.interior[i] + 1u;
+            w.sinter[s] = inter;
+        }
+        // a superset of merge_eligible's particles, whichever way the capacity
+        // guard decides this step's splits (a split particle becomes level 2)
+        if (c.use_merge && c.merge_rule != SPH_MERGE_WAVELET_CELL) {
+            const bool l2 = pi.w != 1.0f;
+            bool may;
+            if (c.merge_rule == SPH_MERGE_WAVELET)
+                may = (l2 && split_score(c, energy, surf) < c.merge_criteria) ||
+                      (split && split_score(c, c.split_ways == 4 ? energy / 4.0f : energy, surf) < c.merge_criteria);
+            else
+                may = (l2 || split) && inter >= c.merge_interior_steps;
+            if (may) atomicAdd(&cnt->merge_candidates, 1u);
         }
     }
 }
@@ -980,6 +996,8 @@ template <int DIM>
 __device__ __forceinline__ void merge_body(const sph_config &c, Counters *cnt, const CanonPtrs &st,
                                            const WorkPtrs &w, uint32_t ncells, uint32_t cap, MergeSmem *ms)
 {
+    // the energy pass found no candidate (the 2D cell rule is not counted there)
+    if (c.merge_rule != SPH_MERGE_WAVELET_CELL && cnt->merge_candidates == 0u) return;
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -1101,6 +1119,7 @@ template <int DIM>
 __device__ __forceinline__ void merge_sibling_body(const sph_config &c, Counters *cnt, const CanonPtrs &st,
                                                    const WorkPtrs &w)
 {
+    if (cnt->merge_candidates == 0u) return;   // the energy pass found no candidate
     const uint32_t n = cnt->n;
     const uint32_t split_on = cnt->split_off ? 0u : 1u;
     const uint32_t ways = c.split_ways == 4 ? 4u : 2u;
@@ -1169,6 +1188,7 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
         cnt_next->split_off = 0;
         cnt_next->split_flags = 0;
         cnt_next->removed_flags = 0;
+        cnt_next->merge_candidates = 0;
     }
     // one thread per particle index: reads gather from the sorted slot, the
     // writes (survivors keep their order) stay coalesced

@@ -95,6 +95,7 @@ __device__ __forceinline__ void write_hash_by_slot_body(const sph_config &c, con
         cnt_next->split_off = 0;
         cnt_next->split_flags = 0;
         cnt_next->removed_flags = 0;
+        cnt_next->merge_candidates = 0;
     }
     const bool inter_rule = c.merge_rule == SPH_MERGE_INTERIOR || c.merge_rule == SPH_MERGE_SIBLING;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -235,7 +236,8 @@ __device__ __forceinline__ bool step_stages(const sph_config &c, Counters *cin, 
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) split_guard_body(c, cin, a.cap);
     if (!grid_barrier(a, ++k, cin, cout)) return false;
-    if (c.use_merge) {
+    // no merge stage when the energy pass found no candidate (read after its barrier)
+    if (c.use_merge && (c.merge_rule == SPH_MERGE_WAVELET_CELL || cin->merge_candidates)) {
         if (c.merge_rule == SPH_MERGE_SIBLING) merge_sibling_body<DIM>(c, cin, in, w);
         else merge_body<DIM>(c, cin, in, w, a.ncells, a.cap, merge);
         if (!grid_barrier(a, ++k, cin, cout)) return false;
