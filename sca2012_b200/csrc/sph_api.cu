@@ -97,6 +97,9 @@ struct sph_handle {
     // config and the step index are the ones it saw
     bool counts_hashed = false;
     uint64_t hashed_gen = 0, hashed_step = 0;
+    // the current state's acc, dens, press, energy and surface are still to be
+    // written from the last step's sorted arrays (k_materialize)
+    bool outputs_pending = false;
     int persist_blocks_per_sm[2][2] = {};    // resident blocks of k_step_persistent<2|3, 64|256> (0: not queried)
     int persist_cluster_ok[2] = {0, 0};      // one-cluster launches: 1 possible, -1 not, 0 not queried
     bool persist_use_cluster = true;         // off: always the polled barriers
@@ -235,6 +238,26 @@ void stage(sph_handle *h, const char *name)
     cudaEventRecord(h->ev[++h->nstages], h->stream);
 }
 
+// Deferred outputs: the ordinary launches record where each output comes
+// from instead of writing acc, dens, press, energy and surface, except under
+// the 2D cell merge rule, whose criterion reads the previous state's energy
+// and surface (beyond the live count too) at merge time.
+static bool defer_outputs(const sph_handle *h)
+{
+    return h->cfg.merge_rule != SPH_MERGE_WAVELET_CELL && h->cap <= kOutSlot;
+}
+
+// Writes the current state's deferred outputs (before anything reads the
+// whole state).
+void ensure_outputs(sph_handle *h)
+{
+    if (!h->outputs_pending) return;
+    const uint32_t G = grid_for(h, h->n_ub);
+    if (h->cfg.dim == 3) k_materialize<3><<<G, kThreads, 0, h->stream>>>(h->cfg, h->cnt + h->cur, h->buf[h->cur], h->w);
+    else k_materialize<2><<<G, kThreads, 0, h->stream>>>(h->cfg, h->cnt + h->cur, h->buf[h->cur], h->w);
+    h->outputs_pending = false;
+}
+
 // The cell counts, keys and slots hold the hash of the current state: the
 // step that wrote it hashed it (its write-out), and nothing has changed the
 // state, the config or the counts since.
@@ -270,6 +293,7 @@ template <int DIM> int run_step(sph_handle *h, bool prologue = true)
     if (c.walk_only) {   // the same pairs found by the stencil walks
         w.nlist = w.ncnt = nullptr;
     }
+    if (!defer_outputs(h)) w.out_src = nullptr;
     cudaStream_t s = h->stream;
     h->nstages = 0;
     if (h->profiling) cudaEventRecord(h->ev[0], s);
@@ -338,6 +362,7 @@ template <int DIM> int run_step(sph_handle *h, bool prologue = true)
     h->counts_hashed = true;   // the write-out hashed the new state
     h->hashed_gen = h->state_gen;
     h->hashed_step = h->step_index;
+    h->outputs_pending = w.out_src != nullptr;
     uint64_t ub = h->n_ub;
     if (c.use_split) ub *= (c.split_ways == 4 ? 4u : 2u);
     h->n_ub = (uint32_t)std::min<uint64_t>(ub, h->cap);
@@ -388,6 +413,7 @@ template <int DIM> int launch_persistent_cluster(sph_handle *h, int &cluster_ok,
     h->w.pos_comp = c.compensated_positions ? 1u : 0u;
     WorkPtrs w = h->w;
     if (c.walk_only) w.nlist = w.ncnt = nullptr;
+    w.out_src = nullptr;   // the persistent step writes every output
     // the polled barriers' state is not used; the one due next is left as it
     // is (clean), so polled launches that follow keep alternating correctly
     PersistArgs a = {};
@@ -418,6 +444,7 @@ template <int DIM, int BS> int launch_persistent(sph_handle *h, int &per_sm, uin
     h->w.pos_comp = c.compensated_positions ? 1u : 0u;
     WorkPtrs w = h->w;
     if (c.walk_only) w.nlist = w.ncnt = nullptr;
+    w.out_src = nullptr;   // the persistent step writes every output
     auto kern = k_step_persistent<DIM, BS>;
     if (per_sm == 0) {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BS, 0) != cudaSuccess || per_sm < 1) {
@@ -476,6 +503,7 @@ template <int DIM> int run_step_persistent(sph_handle *h, int nsteps)
     // state into them
     h->counts_zero = false;
     h->counts_hashed = true;
+    h->outputs_pending = false;
     h->last_launches += 1;
     h->cur = (p + nsteps) & 1;
     h->step_index += (uint64_t)nsteps;
@@ -535,6 +563,7 @@ void write_n(sph_handle *h, uint32_t n)
     cudaMemsetAsync(h->gsync, 0, sizeof(GridSync) * 2, h->stream);
     h->counts_zero = false;
     h->counts_hashed = false;
+    h->outputs_pending = false;   // the caller wrote every field
     cudaStreamSynchronize(h->stream);
 }
 
@@ -588,6 +617,7 @@ int sph_create(const sph_config *cfg, sph_handle **out)
     rc |= dalloc(h, &w.stv, cap); rc |= dalloc(h, &w.sscene, cap);
     rc |= dalloc(h, &w.spos_lo, cap); rc |= dalloc(h, &w.spos_lo_n, cap);
     rc |= dalloc(h, &w.fnb_a, cap); rc |= dalloc(h, &w.fnb_b, cap);
+    rc |= dalloc(h, &w.out_src, cap);
     // neighbour candidate lists (512 B per particle of capacity); without
     // them (very large capacities) the force and energy kernels walk the
     // stencil themselves
@@ -663,6 +693,7 @@ int sph_set_config(sph_handle *h, const sph_config *cfg)
         h->err = "sph_set_config: density grid is fixed at creation";
         return SPH_ERR_INVALID;
     }
+    ensure_outputs(h);   // the last step's outputs, under the config it ran with
     if (cfg->compensated_positions && !h->cfg.compensated_positions) {
         // the low parts start from zero when compensation is switched on
         sph_readback_wait(h);
@@ -690,6 +721,7 @@ int sph_add_particles(sph_handle *h, uint32_t n, const float *pos, const float *
 {
     if (!h || (n && (!pos || !level))) return SPH_ERR_INVALID;
     sph_readback_wait(h);   // the current buffer may still be read back
+    ensure_outputs(h);      // the particles already there keep their outputs
     const int dim = (int)h->cfg.dim;
     uint32_t n0 = read_n(h);
     if ((uint64_t)n0 + n > h->cap) { h->err = "sph_add_particles: capacity exceeded"; return SPH_ERR_CAPACITY; }
@@ -779,7 +811,7 @@ static int capture_step(sph_handle *h)
     const int p = h->cur;
     const uint64_t step_index = h->step_index;
     const uint32_t n_ub = h->n_ub, launches = h->last_launches;
-    const bool counts_zero = h->counts_zero, counts_hashed = h->counts_hashed;
+    const bool counts_zero = h->counts_zero, counts_hashed = h->counts_hashed, pending = h->outputs_pending;
     const uint64_t hashed_gen = h->hashed_gen, hashed_step = h->hashed_step;
     cudaGraph_t g = nullptr;
     h->last_launches = 0;
@@ -794,6 +826,7 @@ static int capture_step(sph_handle *h)
     h->last_launches = launches;
     h->counts_zero = counts_zero;
     h->counts_hashed = counts_hashed;
+    h->outputs_pending = pending;
     h->hashed_gen = hashed_gen;
     h->hashed_step = hashed_step;
     if (rc) return rc;
@@ -853,6 +886,7 @@ int sph_step(sph_handle *h, int nsteps)
             h->counts_hashed = true;
             h->hashed_gen = h->state_gen;
             h->hashed_step = h->step_index;
+            h->outputs_pending = defer_outputs(h);
             uint64_t ub = h->n_ub;
             if (h->cfg.use_split) ub *= (h->cfg.split_ways == 4 ? 4u : 2u);
             h->n_ub = (uint32_t)std::min<uint64_t>(ub, h->cap);
@@ -1010,6 +1044,7 @@ int sph_get_num_particles(sph_handle *h, uint32_t *n)
 int sph_get_state(sph_handle *h, sph_state_view *st)
 {
     if (!h || !st) return SPH_ERR_INVALID;
+    ensure_outputs(h);
     const uint32_t n = read_n(h);
     const uint32_t lim = st->n;   // caller's capacity; 0 = just report n
     st->n = n;
@@ -1106,6 +1141,7 @@ int sph_read_particles(sph_handle *h, void *host_dst, uint64_t capacity_bytes, u
 {
     if (!h || !n_out) return SPH_ERR_INVALID;
     if (int rc = ensure_aos(h)) return rc;
+    ensure_outputs(h);
     const uint32_t n = read_n(h);
     const uint64_t rec = sph_particle_record_size(h);
     *n_out = n;
@@ -1166,6 +1202,7 @@ int sph_read_particles_async(sph_handle *h, void *mapped_dst, uint64_t capacity_
     const int p = h->cur;
     const uint64_t rec = sph_particle_record_size(h);
     const uint32_t max_rec = (uint32_t)std::min<uint64_t>(capacity_bytes / rec, h->cap);
+    ensure_outputs(h);
     cudaEventRecord(h->rb_ready, h->stream);
     cudaStreamWaitEvent(h->rb_stream, h->rb_ready, 0);
     // a few blocks keep PCIe busy; the rest of the GPU stays with the next step
@@ -1418,6 +1455,7 @@ int sph_autotune(sph_handle *h, uint32_t reps, sph_tuning *out)
         c1(d.interior, src.interior, 4ull * n); c1(d.scene, src.scene, 4ull * n);
         c1(d.pos_lo, src.pos_lo, 16ull * n); c1(d.sibling, src.sibling, 4ull * n);
     };
+    ensure_outputs(h);
     copy(save, h->buf[h->cur]);
     const int cur0 = h->cur;
     const uint64_t step0 = h->step_index;
@@ -1428,6 +1466,7 @@ int sph_autotune(sph_handle *h, uint32_t reps, sph_tuning *out)
     sph_set_profiling(h, 1);
     auto restore = [&]() {
         h->counts_hashed = false;
+        h->outputs_pending = false;   // the saved state has every output
         h->cur = cur0;
         copy(h->buf[h->cur], save);
         Counters c0;

@@ -87,7 +87,18 @@ struct WorkPtrs {
     uint32_t nl_stride;                  // slots per list chunk row (the capacity)
     float4 *fnb_a, *fnb_b;               // a force neighbour in two loads: (x, y, z, p/rho^2) and
                                          // (m/rho with the sign bit set for level 2, ev.xyz), by the density pass
+    uint32_t *out_src;                   // deferred outputs: per output index its sorted slot and kOut* flags
+                                         // (nullptr: the write-out writes acc, dens, press, energy, surface)
 };
+
+// Deferred outputs.  acc, dens, press, energy and surface are outputs only:
+// no stage of the next step reads them.  With w.out_src set the write-out
+// records, per output index, the sorted slot its values come from (and how:
+// a split parent, a child, a merge leader), and k_materialize writes the five
+// fields from the step's sorted arrays when something reads the state; the
+// values are write_body's.
+constexpr uint32_t kOutChild = 1u << 31, kOutSplit = 1u << 30, kOutLeader = 1u << 29;
+constexpr uint32_t kOutSlot = (1u << 29) - 1u;
 
 // Neighbour candidates the density pass records per particle: every stencil
 // neighbour within (1 + kNbrListMargin) h_max of the start-of-step position,
@@ -1198,16 +1209,12 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
         const uint32_t rm = ranks ? w.removed_c[i] : 0u;
         const uint32_t rr = ranks ? w.removed_rank[i] : 0u;
         const uint32_t dst = rm ? n_live + rr : i - rr;
-        float4 p = w.spos_n[s], v = w.svel_n[s], e = w.sev_n[s], a = w.sacc_n[s];
-        const float4 aux = w.saux[s];
-        float en = w.senergy[s];
-        const float sf = w.ssurf[s];
+        float4 p = w.spos_n[s], v = w.svel_n[s], e = w.sev_n[s];
         uint32_t inter = (c.merge_rule == SPH_MERGE_INTERIOR || c.merge_rule == SPH_MERGE_SIBLING) ? w.sinter[s] : 0u;
         const float4 p_pre = p;
         if (sp) {
             p.x += hs2;
             p.w = 2.0f;
-            if (ways == 4) en = en / 4.0f;
             inter = 0u;
         }
         float4 plo = w.pos_comp ? w.spos_lo_n[s] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1218,15 +1225,28 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
             if (j < n) sib = j - (ranks ? w.removed_rank[j] : 0u);
         }
         if (sp) sib = n - n_removed + w.split_rank[i] * extra;   // the first child
-        if (w.leader[s]) {
+        const uint32_t leader = w.leader[s];
+        if (leader) {
             plo = make_float4(0.f, 0.f, 0.f, 0.f);   // a merged position is a fresh FP32 mean
-            p = w.mpos[s]; v = w.mvel[s]; e = w.mev[s]; a = w.macc[s];
-            if (DIM == 2) en = w.menergy[s];
+            p = w.mpos[s]; v = w.mvel[s]; e = w.mev[s];
             inter = 0u;
             w.leader[s] = 0u;   // reset for the next step
         }
-        out.pos[dst] = p; out.vel[dst] = v; out.ev[dst] = e; out.acc[dst] = a;
-        out.dens[dst] = aux.x; out.press[dst] = aux.y; out.energy[dst] = en; out.surface[dst] = sf;
+        out.pos[dst] = p; out.vel[dst] = v; out.ev[dst] = e;
+        if (w.out_src) {
+            if (!rm) w.out_src[dst] = s | (sp ? kOutSplit : 0u) | (leader ? kOutLeader : 0u);
+        } else {
+            const float4 aux = w.saux[s];
+            float en = w.senergy[s];
+            if (sp && ways == 4) en = en / 4.0f;
+            float4 a = w.sacc_n[s];
+            if (leader) {
+                a = w.macc[s];
+                if (DIM == 2) en = w.menergy[s];
+            }
+            out.acc[dst] = a; out.dens[dst] = aux.x; out.press[dst] = aux.y; out.energy[dst] = en;
+            out.surface[dst] = w.ssurf[s];
+        }
         out.interior[dst] = inter;
         out.sibling[dst] = sib;
         const uint32_t sid = w.nscenes ? w.sscene[s] : 0u;   // a merge group never spans scenes
@@ -1235,8 +1255,7 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
         if (hash_next && !rm) hash_one<DIM>(c, w, dst, p);
         if (sp) {
             const uint32_t base = n - n_removed + w.split_rank[i] * extra;
-            const float4 v0 = w.svel_n[s], e0 = w.sev_n[s], a0 = w.sacc_n[s];
-            const float ec = ways == 4 ? w.senergy[s] / 4.0f : w.senergy[s];
+            const float4 v0 = w.svel_n[s], e0 = w.sev_n[s];
             for (uint32_t k = 0; k < extra; ++k) {
                 float4 pc = p_pre;
                 pc.w = 2.0f;
@@ -1244,8 +1263,14 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
                 else if (k == 1) pc.z = p_pre.z - hs2;
                 else pc.z = p_pre.z + hs2;
                 const uint32_t cd = base + k;
-                out.pos[cd] = pc; out.vel[cd] = v0; out.ev[cd] = e0; out.acc[cd] = a0;
-                out.dens[cd] = aux.x; out.press[cd] = aux.y; out.energy[cd] = ec; out.surface[cd] = sf;
+                out.pos[cd] = pc; out.vel[cd] = v0; out.ev[cd] = e0;
+                if (w.out_src) {
+                    w.out_src[cd] = s | kOutChild;
+                } else {
+                    const float4 aux = w.saux[s];
+                    out.acc[cd] = w.sacc_n[s]; out.dens[cd] = aux.x; out.press[cd] = aux.y;
+                    out.energy[cd] = ways == 4 ? w.senergy[s] / 4.0f : w.senergy[s]; out.surface[cd] = w.ssurf[s];
+                }
                 out.interior[cd] = 0u;
                 out.sibling[cd] = k + 1 < extra ? cd + 1 : dst;
                 if (w.nscenes) out.scene[cd] = sid;
@@ -1253,6 +1278,32 @@ __device__ __forceinline__ void write_body(const sph_config &c, const Counters *
                 if (hash_next) hash_one<DIM>(c, w, cd, pc);
             }
         }
+    }
+}
+
+// The deferred outputs of the state st (count cnt->n) from the sorted arrays
+// of the step that wrote it, as write_body writes them.
+template <int DIM>
+__global__ void __launch_bounds__(kThreads) k_materialize(sph_config c, const Counters *__restrict__ cnt,
+                                                         CanonPtrs st, WorkPtrs w)
+{
+    const uint32_t n = cnt->n;
+    const uint32_t ways = c.split_ways == 4 ? 4u : 2u;
+    for (uint32_t i = grid_stride_start(); i < n; i += grid_stride()) {
+        const uint32_t code = w.out_src[i], s = code & kOutSlot;
+        const float4 aux = w.saux[s];
+        float en = w.senergy[s];
+        float4 a = w.sacc_n[s];
+        if (code & kOutChild) {
+            en = ways == 4 ? en / 4.0f : en;
+        } else {
+            if ((code & kOutSplit) && ways == 4) en = en / 4.0f;
+            if (code & kOutLeader) {
+                a = w.macc[s];
+                if (DIM == 2) en = w.menergy[s];
+            }
+        }
+        st.acc[i] = a; st.dens[i] = aux.x; st.press[i] = aux.y; st.energy[i] = en; st.surface[i] = w.ssurf[s];
     }
 }
 

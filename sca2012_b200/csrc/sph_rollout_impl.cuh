@@ -111,11 +111,13 @@ int restore_ckpt(sph_handle *h, Rollout *r, size_t k)
     cudaStreamSynchronize(h->stream);
     h->n_ub = n;
     h->counts_hashed = false;   // the hash a persistent step left is not this state's
+    h->outputs_pending = false;
     return cuda_check(h, "rollout: restore checkpoint");
 }
 
 int save_ckpt(sph_handle *h, Rollout *r, size_t k)
 {
+    ensure_outputs(h);
     const uint32_t n = read_n(h);
     copy_canon(r->ckpt[k], h->buf[h->cur], n, h->stream);
     r->ckpt_n[k] = n;
